@@ -1,0 +1,62 @@
+/*
+ * mublis_b200.h -- B200-specific extensions of libmublis.
+ *
+ * None of these has a counterpart in the reference (a CPU library with no
+ * device, streams or precision forms); they sit beside the unchanged
+ * cblas.h / mublis.h entry points.  All return 0 on success, nonzero on
+ * failure (1 invalid argument, 2 CUDA failure, 3 out of memory / refused,
+ * 4 a bounded device wait gave up); mublis_b200_last_error() describes the
+ * calling thread's last failure.
+ */
+#ifndef MUBLIS_B200_H
+#define MUBLIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "mublis.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Brings up the device (also done lazily by the first call).  Fails when no
+ * sm_100 device is present: the library has no CPU fallback. */
+int mublis_b200_init(void);
+const char *mublis_b200_last_error(void);
+
+/* Per-thread stream.  Each host thread gets its own non-blocking stream by
+ * default; set_stream makes the library issue the calling thread's work on
+ * the given cudaStream_t instead (the caller keeps ownership).  Calls remain
+ * synchronous: they return after their work on that stream completes. */
+int mublis_b200_set_stream(void *cuda_stream);
+void *mublis_b200_get_stream(void);
+
+/* Precision form used by the routines of one precision ('s' or 'd'):
+ *   's': "plain" (FP32 FMA pipe), "bf16x3" (tcgen05, hi/lo split, 3
+ *        products, FP32 accumulate), "bf16x6" (3-term split, 6 products)
+ *   'd': "plain" (FP64 FMA pipe), "ozaki" or "ozaki:<slices>" (int8 slices,
+ *        exact int32 tensor-core accumulation, FP64 recombination)
+ * Also settable with MUBLIS_B200_SFORM / MUBLIS_B200_DFORM. */
+int mublis_b200_set_form(char dtype, const char *form);
+
+/* Launch accounting and per-kernel device timing.  profile_read writes
+ * {"kernel": [launches, total_ms], ...} for launches since the last read. */
+unsigned long long mublis_b200_launch_count(void);
+int mublis_b200_profile_enable(int on);
+int mublis_b200_profile_read(char *buf, unsigned long len);
+
+/* Seeded device fills (Philox4x32-10, key = (seed, matrix_id), counter =
+ * column-major element index i + j*m; kind 0 uniform[-1,1), 1 wide
+ * +-[1,2)*2^[-10,10], 2 uniform[1,2)).  x is a device pointer to an m x n
+ * column-major matrix with leading dimension ld. */
+int mublis_b200_fill_s(float *x, long m, long n, long ld, uint32_t seed, uint32_t matrix_id,
+                       int kind);
+int mublis_b200_fill_d(double *x, long m, long n, long ld, uint32_t seed, uint32_t matrix_id,
+                       int kind);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

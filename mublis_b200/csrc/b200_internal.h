@@ -1,0 +1,115 @@
+/*
+ * b200_internal.h -- C-ABI between the C host layer (cblas, BLAS shims,
+ * driver front-end, context) and the CUDA side of libmublis.
+ *
+ * Everything below takes DEVICE pointers: the host layer resolves caller
+ * memory (host buffers are staged, device buffers are used in place) before
+ * calling in.  All work is issued on the calling thread's library stream;
+ * b200_stream_sync() makes it visible.
+ */
+#ifndef MUBLIS_B200_INTERNAL_H
+#define MUBLIS_B200_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/mublis.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  B200_OK = 0,
+  B200_EINVAL = 1, /* bad argument or unsupported request */
+  B200_ECUDA = 2,  /* a CUDA call failed (no device, launch error, ...) */
+  B200_ENOMEM = 3, /* device or pinned allocation failed, or admission refused */
+  B200_ETIMEOUT = 4 /* a bounded device-side wait gave up */
+};
+
+enum { B200_F32 = 0, B200_F64 = 1 };
+
+/* Arithmetic form of the contraction.  PLAIN: FP32/FP64 FMA pipes.
+ * BF16X3: FP32 operands split into bf16 hi+lo, three tcgen05 products per
+ * k-block accumulated in FP32 (hi*hi + hi*lo + lo*hi).  BF16X6: three-term
+ * split, six products.  OZAKI: FP64 via int8 slices with exact int32
+ * accumulation (slice count in b200_form_t.slices). */
+enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM_BF16X6 = 2,
+       B200_FORM_OZAKI = 3 };
+
+/* One product C(ji) := alpha * sum_t A_t B_t + beta * C over the domain of
+ * `product`.  npairs is 1, or 2 for SYR2K (both pairs share the product's
+ * operand structure and are concatenated along k). */
+typedef struct {
+  int dtype;
+  int m, n, k;
+  double alpha, beta;
+  int npairs;
+  const void *a[2];
+  long rs_a[2], cs_a[2];
+  const void *b[2];
+  long rs_b[2], cs_b[2];
+  void *c;
+  long rs_c, cs_c;
+  mublis_l3_product_t product;
+  int form;   /* B200_FORM_* or AUTO (library default for the dtype) */
+  int slices; /* Ozaki slice count, 0 = library default */
+} b200_l3_desc_t;
+
+/* Left-side solve op(A) X = alpha B, already normalised by the host layer
+ * (side RIGHT and trans folded into strides/uplo as trsm.c:35-54 does). */
+typedef struct {
+  int dtype;
+  int m, n;
+  double alpha;
+  const void *a;
+  long rs_a, cs_a;
+  void *b;
+  long rs_b, cs_b;
+  mublis_uplo_t uplo; /* LOWER or UPPER of op(A) */
+  int unit_diag;
+  int form;
+  int slices;
+} b200_trsm_desc_t;
+
+/* runtime.cu */
+int b200_init(void);
+int b200_device_count(void);
+int b200_is_device_ptr(const void *p);
+void *b200_stream(void);
+int b200_set_thread_stream(void *stream);
+int b200_stream_sync(void);
+int b200_alloc(void **p, size_t bytes);
+void b200_free(void *p);
+int b200_set_error(int code, const char *where);
+const char *b200_last_error(void);
+int b200_get_default_form(int dtype);
+int b200_set_default_form(int dtype, int form, int slices);
+int b200_get_default_slices(void);
+
+/* Strided copies between caller host memory and a compact device buffer of
+ * rows x cols with leading dimension ld (column-major).  The host side may
+ * have any (rs, cs). */
+int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long rows, long cols,
+                  size_t elt);
+int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,
+                  size_t elt);
+
+/* l3.cu */
+int b200_l3_run(const b200_l3_desc_t *d);
+int b200_trsm_run(const b200_trsm_desc_t *d);
+int b200_scale_strided(int dtype, int m, int n, double beta, void *c, long rs, long cs,
+                       mublis_l3_relation_t ji);
+
+/* ukr.cu: one MR x NR micro-tile on the device (packed host panels). */
+int b200_ukr_gemm(int dtype, int k, const void *alpha, const void *a, const void *b,
+                  const void *beta, void *c, int rs_c, int cs_c, int mr, int nr);
+int b200_ukr_gemmtrsm(int dtype, int lower, int k, const void *alpha, const void *a1x,
+                      const void *a11, const void *bx1, void *b11, void *c11, int rs_c,
+                      int cs_c, int mr, int nr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,228 @@
+// gemm_simt.cu -- plain FP32 / FP64 GEMM on the FMA pipes: the device
+// form of the reference's five-loop driver (frame/l3/l3_driver.c:126-239)
+// plus its micro-kernel (include/mublis_instantiate.h:37-52).
+//
+// One CTA per output tile (BM x BN), 256 threads, each thread an 8 x TN
+// register tile laid out CUTLASS-SIMT style (4 x 8 threads per warp, 4-wide
+// fragments) so every shared-memory fragment load is a broadcast or a single
+// 128-byte wavefront.  Operands come from packed MN-major panels (pack.cu)
+// through a STAGES-deep cp.async pipeline; packing zero-pads every edge, so
+// the main loop has no bounds checks.
+//
+// Domain handling replaces the reference's block pruning:
+//   ji  -- tiles wholly outside the written triangle exit at once
+//          (block_is_outside, l3_driver.c:145-147,165-171); partial tiles
+//          are masked element-wise in the epilogue (:217-233);
+//   jp, pi -- the tile's k-range is clipped to the product's support
+//          (:130,148-150,163,171), e.g. TRMM does half the work of GEMM.
+// Epilogue: C = alpha*acc + beta*C, and beta == 0 never reads C
+// (:111-112, :224-225).  A tile with an empty k-range writes beta*C, which is
+// the reference's "no update" pass (:88-121).
+#include "kernels.cuh"
+
+namespace {
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void lds4(float (&d)[4], const float *p) {
+  float4 v = *reinterpret_cast<const float4 *>(p);
+  d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+}
+__device__ __forceinline__ void lds4(double (&d)[4], const double *p) {
+  double2 v0 = *reinterpret_cast<const double2 *>(p);
+  double2 v1 = *reinterpret_cast<const double2 *>(p + 2);
+  d[0] = v0.x; d[1] = v0.y; d[2] = v1.x; d[3] = v1.y;
+}
+
+template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB>
+__global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p) {
+  constexpr int NT = 256;
+  constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;
+  constexpr int TM = WTM / 4, TN = WTN / 8;
+  constexpr int MCH = TM / 4, NCH = TN / 4;
+  constexpr int MSP = WTM / MCH, NSP = WTN / NCH;  // chunk spacing
+  constexpr int VEC = 16 / sizeof(T);
+  static_assert(WARPS_M * WARPS_N == 8, "8 warps");
+  static_assert(TM % 4 == 0 && TN % 4 == 0, "4-wide fragments");
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *As = reinterpret_cast<T *>(smem_raw);
+  T *Bs = As + STAGES * BK * BM;
+
+  // Rasterise tiles in groups of 8 along M for L2 reuse of B panels.
+  const int tiles_m = (p.m + BM - 1) / BM, tiles_n = (p.n + BN - 1) / BN;
+  const int bid = blockIdx.x;
+  constexpr int G = 8;
+  const int group = bid / (G * tiles_n);
+  const int first_m = group * G;
+  const int gsize = min(tiles_m - first_m, G);
+  const int in_group = bid % (G * tiles_n);
+  const int tm = first_m + in_group % gsize, tn = in_group / gsize;
+  const long m0 = (long)tm * BM, n0 = (long)tn * BN;
+
+  // block_is_outside(ji, n0, BN, m0, BM)
+  if (p.ji == MUBLIS_L3_LOWER && n0 >= m0 + BM) return;
+  if (p.ji == MUBLIS_L3_UPPER && n0 + BN <= m0) return;
+
+  long kb = 0, ke = p.k;
+  if (p.jp == MUBLIS_L3_LOWER) kb = max(kb, n0);       // j <= p
+  if (p.jp == MUBLIS_L3_UPPER) ke = min(ke, n0 + BN);  // j >= p
+  if (p.pi == MUBLIS_L3_LOWER) ke = min(ke, m0 + BM);  // p <= i
+  if (p.pi == MUBLIS_L3_UPPER) kb = max(kb, m0);       // p >= i
+  const int kt_begin = (int)(kb / BK);
+  const int kt_end = ke > kb ? (int)((ke + BK - 1) / BK) : kt_begin;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp % WARPS_M, wn = warp / WARPS_M;
+  const int ty = lane >> 3, tx = lane & 7;
+
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+  auto load_stage = [&](int stage, int kt) {
+    const T *ga = p.ap + (long)kt * BK * p.lda + m0;
+    const T *gb = p.bp + (long)kt * BK * p.ldb + n0;
+    T *sa = As + stage * BK * BM;
+    T *sb = Bs + stage * BK * BN;
+#pragma unroll
+    for (int c = tid; c < BK * BM / VEC; c += NT) {
+      int row = c / (BM / VEC), col = (c % (BM / VEC)) * VEC;
+      cp_async16(sa + row * BM + col, ga + (long)row * p.lda + col);
+    }
+#pragma unroll
+    for (int c = tid; c < BK * BN / VEC; c += NT) {
+      int row = c / (BN / VEC), col = (c % (BN / VEC)) * VEC;
+      cp_async16(sb + row * BN + col, gb + (long)row * p.ldb + col);
+    }
+  };
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (kt_begin + s < kt_end) load_stage(s, kt_begin + s);
+    cp_async_commit();
+  }
+
+  for (int kt = kt_begin; kt < kt_end; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int nk = kt + STAGES - 1;
+    if (nk < kt_end) load_stage((nk - kt_begin) % STAGES, nk);
+    cp_async_commit();
+
+    const int st = (kt - kt_begin) % STAGES;
+    const T *sa = As + st * BK * BM + wm * WTM + ty * 4;
+    const T *sb = Bs + st * BK * BN + wn * WTN + tx * 4;
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T af[TM], bf[TN];
+#pragma unroll
+      for (int mc = 0; mc < MCH; ++mc) {
+        T t[4];
+        lds4(t, sa + kk * BM + mc * MSP);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) af[mc * 4 + q] = t[q];
+      }
+#pragma unroll
+      for (int nc = 0; nc < NCH; ++nc) {
+        T t[4];
+        lds4(t, sb + kk * BN + nc * NSP);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bf[nc * 4 + q] = t[q];
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  const T alpha = p.alpha, beta = p.beta;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const long gi = m0 + wm * WTM + (i / 4) * MSP + ty * 4 + (i % 4);
+    if (gi >= p.m) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + wn * WTN + (j / 4) * NSP + tx * 4 + (j % 4);
+      if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
+      T *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+      T v = alpha * acc[i][j];
+      if (beta != T(0)) v = fma(beta, *cij, v);
+      *cij = v;
+    }
+  }
+}
+
+template <typename T>
+__global__ void scale_kernel(int m, int n, T beta, T *c, long rs, long cs, int ji) {
+  long total = (long)m * n;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    long i, j;
+    if (rs <= cs) { i = t % m; j = t / m; } else { j = t % n; i = t / n; }
+    if (!b200_rel(ji, j, i)) continue;
+    T *cij = c + i * rs + j * cs;
+    *cij = beta == T(0) ? T(0) : beta * *cij;
+  }
+}
+
+template <typename T>
+struct SimtTraits;
+template <>
+struct SimtTraits<float> {
+  static constexpr int WARPS_M = 4, WARPS_N = 2, STAGES = 4, MINB = 2;
+};
+template <>
+struct SimtTraits<double> {
+  static constexpr int WARPS_M = 4, WARPS_N = 2, STAGES = 4, MINB = 2;
+};
+
+}  // namespace
+
+template <typename T>
+int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s) {
+  using C = SimtConfig<T>;
+  using R = SimtTraits<T>;
+  auto kern = simt_gemm_kernel<T, C::BM, C::BN, C::BK, R::WARPS_M, R::WARPS_N, R::STAGES, R::MINB>;
+  const size_t smem = (size_t)R::STAGES * C::BK * (C::BM + C::BN) * sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  long tiles = b200_ceil_div(a.m, C::BM) * b200_ceil_div(a.n, C::BN);
+  if (tiles <= 0) return B200_OK;
+  if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "gemm: too many tiles");
+  B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
+  kern<<<(unsigned)tiles, 256, smem, s>>>(a);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
+template <typename T>
+int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return B200_OK;
+  long total = (long)m * n;
+  unsigned blocks = (unsigned)std::min<long>(b200_ceil_div(total, 256), 148L * 16);
+  B200ProfScope prof("scale", s);
+  scale_kernel<T><<<blocks, 256, 0, s>>>(m, n, beta, c, rs, cs, ji);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
+template int launch_simt_gemm<float>(const SimtGemmArgs<float> &, cudaStream_t);
+template int launch_simt_gemm<double>(const SimtGemmArgs<double> &, cudaStream_t);
+template int launch_scale<float>(int, int, float, float *, long, long, int, cudaStream_t);
+template int launch_scale<double>(int, int, double, double *, long, long, int, cudaStream_t);

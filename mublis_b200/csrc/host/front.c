@@ -1,0 +1,285 @@
+/*
+ * front.c -- the host side of mublis_l3_{s,d}driver, TRMM and TRSM.
+ *
+ *   mublis_l3_{s,d}driver  include/mublis.h:65-83, reference
+ *                          frame/l3/l3_driver.c:49-256: same arguments, same
+ *                          m == 0 || n == 0 early return (:61-62), status 0 on
+ *                          success.  The descriptor goes to the device driver
+ *                          (l3.cu) instead of the CPU loop nest.
+ *   TRMM front             frame/l3/trmm.c:44-85 (normalisation and product
+ *                          descriptor), :138-144 (alpha == 0 zeroes B)
+ *   TRSM front             frame/l3/trsm.c:24-54 (alpha == 0 zeroes B; right
+ *                          side -> left; trans -> stride swap + flip_uplo)
+ */
+#include "front.h"
+
+#include <string.h>
+
+static int views_same(const b200_stage_t *s, const void *p, long rows, long cols, long rs,
+                      long cs) {
+  return s->host == p && s->rows == rows && s->cols == cols && s->rs == rs && s->cs == cs;
+}
+
+void b200_stage_begin(b200_stage_set_t *ss, size_t elt) {
+  memset(ss, 0, sizeof *ss);
+  ss->elt = elt;
+}
+
+int b200_stage_view(b200_stage_set_t *ss, const void *p, long rows, long cols, long rs, long cs,
+                    int copy_in, int out, b200_view_t *v) {
+  v->ptr = (void *)p;
+  v->rs = rs;
+  v->cs = cs;
+  if (rows <= 0 || cols <= 0) return B200_OK;
+  if (p == NULL) return b200_set_error(B200_EINVAL, "null operand pointer");
+  if (b200_is_device_ptr(p)) return B200_OK;
+
+  for (int q = 0; q < ss->n; ++q) {
+    b200_stage_t *s = &ss->st[q];
+    int same = views_same(s, p, rows, cols, rs, cs);
+    int swapped = views_same(s, p, cols, rows, cs, rs);
+    if (!same && !swapped) continue;
+    s->out |= out;
+    /* Device strides of the staged copy in the requested orientation. */
+    long drs = s->transposed ? s->ld : 1, dcs = s->transposed ? 1 : s->ld;
+    v->ptr = s->dev;
+    v->rs = same ? drs : dcs;
+    v->cs = same ? dcs : drs;
+    return B200_OK;
+  }
+  if (ss->n == (int)(sizeof ss->st / sizeof ss->st[0]))
+    return b200_set_error(B200_EINVAL, "too many staged operands");
+
+  b200_stage_t *s = &ss->st[ss->n];
+  memset(s, 0, sizeof *s);
+  s->host = p;
+  s->rows = rows;
+  s->cols = cols;
+  s->rs = rs;
+  s->cs = cs;
+  s->out = out;
+  s->transposed = rs != 1 && cs == 1;
+  s->ld = s->transposed ? cols : rows;
+  int st = b200_alloc(&s->dev, (size_t)rows * (size_t)cols * ss->elt);
+  if (st != B200_OK) return st;
+  ss->n++;
+  if (copy_in) {
+    st = s->transposed
+             ? b200_copy_h2d(s->dev, s->ld, p, cs, rs, cols, rows, ss->elt)
+             : b200_copy_h2d(s->dev, s->ld, p, rs, cs, rows, cols, ss->elt);
+    if (st != B200_OK) return st;
+  }
+  v->ptr = s->dev;
+  v->rs = s->transposed ? s->ld : 1;
+  v->cs = s->transposed ? 1 : s->ld;
+  return B200_OK;
+}
+
+int b200_stage_end(b200_stage_set_t *ss, int status) {
+  for (int q = 0; q < ss->n && status == B200_OK; ++q) {
+    b200_stage_t *s = &ss->st[q];
+    if (!s->out) continue;
+    status = s->transposed
+                 ? b200_copy_d2h((void *)s->host, s->cs, s->rs, s->dev, s->ld, s->cols, s->rows,
+                                 ss->elt)
+                 : b200_copy_d2h((void *)s->host, s->rs, s->cs, s->dev, s->ld, s->rows, s->cols,
+                                 ss->elt);
+  }
+  int sync = b200_stream_sync();
+  for (int q = 0; q < ss->n; ++q) b200_free(ss->st[q].dev);
+  ss->n = 0;
+  if (status == B200_OK) status = sync;
+  return status;
+}
+
+static size_t elt_of(int dtype) { return dtype == B200_F64 ? sizeof(double) : sizeof(float); }
+
+int b200_front_l3(b200_l3_desc_t *d) {
+  if (d->m == 0 || d->n == 0) return B200_OK;
+  if (d->m < 0 || d->n < 0 || d->k < 0) return b200_set_error(B200_EINVAL, "negative size");
+  int st = b200_init();
+  if (st != B200_OK) return st;
+
+  b200_stage_set_t ss;
+  b200_stage_begin(&ss, elt_of(d->dtype));
+  b200_l3_desc_t dd = *d;
+  const int update = d->alpha != 0.0 && d->k > 0;
+  b200_view_t v;
+  for (int t = 0; t < d->npairs && update && st == B200_OK; ++t) {
+    st = b200_stage_view(&ss, d->a[t], d->m, d->k, d->rs_a[t], d->cs_a[t], 1, 0, &v);
+    dd.a[t] = v.ptr;
+    dd.rs_a[t] = v.rs;
+    dd.cs_a[t] = v.cs;
+    if (st != B200_OK) break;
+    st = b200_stage_view(&ss, d->b[t], d->k, d->n, d->rs_b[t], d->cs_b[t], 1, 0, &v);
+    dd.b[t] = v.ptr;
+    dd.rs_b[t] = v.rs;
+    dd.cs_b[t] = v.cs;
+  }
+  if (st == B200_OK) {
+    /* C is read when beta != 0, and must be preserved outside the written
+     * triangle when ji restricts the output. */
+    int c_in = d->beta != 0.0 || d->product.domain.ji != MUBLIS_L3_ALL;
+    st = b200_stage_view(&ss, d->c, d->m, d->n, d->rs_c, d->cs_c, c_in, 1, &v);
+    dd.c = v.ptr;
+    dd.rs_c = v.rs;
+    dd.cs_c = v.cs;
+  }
+  if (st == B200_OK) st = b200_l3_run(&dd);
+  return b200_stage_end(&ss, st);
+}
+
+static mublis_uplo_t flip(mublis_uplo_t u) {
+  return u == MUBLIS_LOWER ? MUBLIS_UPPER : (u == MUBLIS_UPPER ? MUBLIS_LOWER : MUBLIS_DENSE);
+}
+
+int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_trans_t trans,
+                    mublis_diag_t diag, int m, int n, double alpha, const void *a, int rs_a,
+                    int cs_a, void *b, int rs_b, int cs_b) {
+  if (m == 0 || n == 0) return B200_OK;
+  if (m < 0 || n < 0) return b200_set_error(B200_EINVAL, "negative size");
+  int st = b200_init();
+  if (st != B200_OK) return st;
+  b200_stage_set_t ss;
+  b200_stage_begin(&ss, elt_of(dtype));
+  b200_view_t vb, va;
+  st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  if (st == B200_OK && alpha == 0.0) {
+    st = b200_scale_strided(dtype, m, n, 0.0, vb.ptr, vb.rs, vb.cs, MUBLIS_L3_ALL);
+    return b200_stage_end(&ss, st);
+  }
+  int ka = side == MUBLIS_LEFT ? m : n;
+  if (st == B200_OK) st = b200_stage_view(&ss, a, ka, ka, rs_a, cs_a, 1, 0, &va);
+  if (st != B200_OK) return b200_stage_end(&ss, st);
+
+  long ars = va.rs, acs = va.cs;
+  if (trans == MUBLIS_TRANSPOSE) { /* trmm.c:44-49 */
+    long t = ars; ars = acs; acs = t;
+    uplo = flip(uplo);
+  }
+  mublis_l3_relation_t tri = uplo == MUBLIS_LOWER ? MUBLIS_L3_LOWER : MUBLIS_L3_UPPER;
+  mublis_l3_operand_t gen = {MUBLIS_STRUC_GENERAL, MUBLIS_DENSE, MUBLIS_PACKM_DIAG_NONUNIT};
+  mublis_l3_operand_t trio = {MUBLIS_STRUC_TRIANGULAR, uplo,
+                              diag == MUBLIS_UNIT_DIAG ? MUBLIS_PACKM_DIAG_UNIT
+                                                       : MUBLIS_PACKM_DIAG_NONUNIT};
+  b200_l3_desc_t d;
+  memset(&d, 0, sizeof d);
+  d.dtype = dtype;
+  d.m = m;
+  d.n = n;
+  d.alpha = alpha;
+  d.beta = 0.0;
+  d.npairs = 1;
+  d.form = B200_FORM_AUTO;
+  d.product.domain.ji = MUBLIS_L3_ALL;
+  if (side == MUBLIS_LEFT) { /* trmm.c:51-82,98-106 */
+    d.k = m;
+    d.product.domain.pi = tri;
+    d.product.domain.jp = MUBLIS_L3_ALL;
+    d.product.a = trio;
+    d.product.b = gen;
+    d.a[0] = va.ptr; d.rs_a[0] = ars; d.cs_a[0] = acs;
+    d.b[0] = vb.ptr; d.rs_b[0] = vb.rs; d.cs_b[0] = vb.cs;
+  } else {
+    d.k = n;
+    d.product.domain.jp = tri;
+    d.product.domain.pi = MUBLIS_L3_ALL;
+    d.product.a = gen;
+    d.product.b = trio;
+    d.a[0] = vb.ptr; d.rs_a[0] = vb.rs; d.cs_a[0] = vb.cs;
+    d.b[0] = va.ptr; d.rs_b[0] = ars; d.cs_b[0] = acs;
+  }
+  /* In place: the device driver packs both operands before the contraction
+   * writes C, so C may alias B. */
+  d.c = vb.ptr;
+  d.rs_c = vb.rs;
+  d.cs_c = vb.cs;
+  st = b200_l3_run(&d);
+  return b200_stage_end(&ss, st);
+}
+
+int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_trans_t trans,
+                    mublis_diag_t diag, int m, int n, double alpha, const void *a, int rs_a,
+                    int cs_a, void *b, int rs_b, int cs_b) {
+  if (m == 0 || n == 0) return B200_OK;
+  if (m < 0 || n < 0) return b200_set_error(B200_EINVAL, "negative size");
+  int st = b200_init();
+  if (st != B200_OK) return st;
+  b200_stage_set_t ss;
+  b200_stage_begin(&ss, elt_of(dtype));
+  b200_view_t vb, va;
+  st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  if (st == B200_OK && alpha == 0.0) { /* trsm.c:27-33 */
+    st = b200_scale_strided(dtype, m, n, 0.0, vb.ptr, vb.rs, vb.cs, MUBLIS_L3_ALL);
+    return b200_stage_end(&ss, st);
+  }
+  int ka = side == MUBLIS_LEFT ? m : n;
+  if (st == B200_OK) st = b200_stage_view(&ss, a, ka, ka, rs_a, cs_a, 1, 0, &va);
+  if (st != B200_OK) return b200_stage_end(&ss, st);
+
+  long brs = vb.rs, bcs = vb.cs, ars = va.rs, acs = va.cs;
+  if (side == MUBLIS_RIGHT) { /* trsm.c:35-47 */
+    int t = m; m = n; n = t;
+    long u = brs; brs = bcs; bcs = u;
+    trans = trans == MUBLIS_NO_TRANSPOSE ? MUBLIS_TRANSPOSE : MUBLIS_NO_TRANSPOSE;
+  }
+  if (trans == MUBLIS_TRANSPOSE) { /* trsm.c:49-54 */
+    long u = ars; ars = acs; acs = u;
+    uplo = flip(uplo);
+  }
+  b200_trsm_desc_t d;
+  memset(&d, 0, sizeof d);
+  d.dtype = dtype;
+  d.m = m;
+  d.n = n;
+  d.alpha = alpha;
+  d.a = va.ptr;
+  d.rs_a = ars;
+  d.cs_a = acs;
+  d.b = vb.ptr;
+  d.rs_b = brs;
+  d.cs_b = bcs;
+  d.uplo = uplo;
+  d.unit_diag = diag == MUBLIS_UNIT_DIAG;
+  d.form = B200_FORM_AUTO;
+  st = b200_trsm_run(&d);
+  return b200_stage_end(&ss, st);
+}
+
+/* ---- mublis_l3_{s,d}driver ---------------------------------------------- */
+
+static int driver(int dtype, int m, int n, int k, double alpha, const void *a, int rs_a,
+                  int cs_a, const void *b, int rs_b, int cs_b, double beta, void *c, int rs_c,
+                  int cs_c, const mublis_l3_product_t *product) {
+  if (m == 0 || n == 0) return 0;
+  if (product == NULL) return b200_set_error(B200_EINVAL, "null product descriptor");
+  b200_l3_desc_t d;
+  memset(&d, 0, sizeof d);
+  d.dtype = dtype;
+  d.m = m;
+  d.n = n;
+  d.k = k;
+  d.alpha = alpha;
+  d.beta = beta;
+  d.npairs = 1;
+  d.a[0] = a; d.rs_a[0] = rs_a; d.cs_a[0] = cs_a;
+  d.b[0] = b; d.rs_b[0] = rs_b; d.cs_b[0] = cs_b;
+  d.c = c; d.rs_c = rs_c; d.cs_c = cs_c;
+  d.product = *product;
+  d.form = B200_FORM_AUTO;
+  return b200_front_l3(&d);
+}
+
+int mublis_l3_sdriver(int m, int n, int k, float alpha, const float *a, int rs_a, int cs_a,
+                      const float *b, int rs_b, int cs_b, float beta, float *c, int rs_c,
+                      int cs_c, const mublis_l3_product_t *product) {
+  return driver(B200_F32, m, n, k, alpha, a, rs_a, cs_a, b, rs_b, cs_b, beta, c, rs_c, cs_c,
+                product);
+}
+
+int mublis_l3_ddriver(int m, int n, int k, double alpha, const double *a, int rs_a, int cs_a,
+                      const double *b, int rs_b, int cs_b, double beta, double *c, int rs_c,
+                      int cs_c, const mublis_l3_product_t *product) {
+  return driver(B200_F64, m, n, k, alpha, a, rs_a, cs_a, b, rs_b, cs_b, beta, c, rs_c, cs_c,
+                product);
+}

@@ -1,0 +1,79 @@
+// kernels.cuh -- launchers shared between the CUDA translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+// Logical operand view for packing.  Element (r, c) of the stored operand
+// lives at x[r * rs + c * cs]; `struc/uplo/diag` give its logical view
+// (frame/l1m/packm.c:40-71) and `mask_rel` a domain relation applied as
+// rel(mask_rel, c, r) (pi on A's (i, p) or jp on B's (p, j)).
+struct PackView {
+  const void *x;
+  long rs, cs;
+  int struc, uplo, diag;
+  int mask_rel;
+};
+
+// Output orientation of a packed panel.  The panel covers mn in [0, mn_pad)
+// and kk in [kk0, kk1); logical element (mn, kk - kk0) is taken from the
+// view, as (r, c) = (mn, kk) for an A-side view or (kk, mn) for a B-side
+// view; anything past mn_len / k_len is zero.
+enum PackLayout {
+  PACK_MN_MAJOR = 0,  // out[kk * ld + mn]       (SIMT kernels)
+  PACK_K_MAJOR = 1    // out[mn * ld + kk]       (tcgen05 kernels)
+};
+
+enum PackXform {
+  PACK_COPY = 0,       // T -> T
+  PACK_BF16_SPLIT = 1  // f32 -> `terms` bf16 planes (hi, lo[, lo2])
+};
+
+struct PackOut {
+  void *out;
+  long ld;
+  long plane_stride;  // elements between bf16 planes
+  int layout, xform, terms;
+};
+
+template <typename T>
+int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn_pad,
+                long kk0, long kk1, const PackOut &o, cudaStream_t s);
+
+// Plain FP32 / FP64 GEMM on the FMA pipes over packed MN-major panels.
+template <typename T>
+struct SimtGemmArgs {
+  const T *ap;  // [Kpad][Mpad]
+  const T *bp;  // [Kpad][Npad]
+  long lda, ldb;
+  T *c;
+  long rs_c, cs_c;
+  int m, n, k;
+  T alpha, beta;
+  int jp, ji, pi;
+};
+
+template <typename T>
+struct SimtConfig;
+
+template <>
+struct SimtConfig<float> {
+  static constexpr int BM = 128, BN = 128, BK = 16;
+};
+template <>
+struct SimtConfig<double> {
+  static constexpr int BM = 128, BN = 64, BK = 16;
+};
+
+template <typename T>
+int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s);
+
+template <typename T>
+int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStream_t s);
+
+// Diagonal-block solve of a left TRSM: rows [0, mb) of B (mb <= 64) solved
+// against the mb x mb triangle at a (op applied via strides), in place.
+template <typename T>
+int launch_trsm_leaf(int mb, int n, const T *a, long rs_a, long cs_a, T *b, long rs_b, long cs_b,
+                     bool lower, bool unit, cudaStream_t s);

@@ -1,0 +1,113 @@
+// pack.cu -- the device counterpart of the reference's packm
+// (frame/l1m/packm.c:18-84).
+//
+// The reference copies MR/NR micro-panels into cache-sized buffers, resolving
+// op() (stride swap), symmetric reflection (:50-58) and triangular zero /
+// unit / inverted diagonals (:60-71) element by element.  On the B200 the
+// same logical view is resolved in one HBM pass per operand into a padded,
+// canonical panel that the GEMM kernels stream with 16-byte (SIMT) or TMA
+// (tcgen05) loads and never bounds-check:
+//   * 32 x 32 tiles go through shared memory so that both the source read
+//     (along whichever source stride is 1) and the panel write are coalesced;
+//   * the domain relation of the generic driver (pi for A, jp for B) is
+//     applied here as structural zeros, which makes the driver's result
+//     element-wise well defined for any domain/structure combination;
+//   * for the tensor-core forms the FP32 value is split into bf16 planes
+//     (hi = rn(x), lo = rn(x - hi), lo2 = rn(x - hi - lo)) in the same pass.
+// Elements outside the stored triangle of a structured operand are never
+// read (the reference's tests poison them with NaN).
+#include "kernels.cuh"
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T load_logical(const PackView &v, long r, long c) {
+  const T *x = (const T *)v.x;
+  if (!b200_rel(v.mask_rel, c, r)) return T(0);
+  long delta = r - c;
+  bool stored = v.uplo == MUBLIS_LOWER ? delta >= 0 : (v.uplo == MUBLIS_UPPER ? delta <= 0 : true);
+  if (v.struc == MUBLIS_STRUC_SYMMETRIC) {
+    return stored ? x[r * v.rs + c * v.cs] : x[c * v.rs + r * v.cs];
+  }
+  if (v.struc == MUBLIS_STRUC_TRIANGULAR) {
+    if (!stored) return T(0);
+    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_UNIT) return T(1);
+    T val = x[r * v.rs + c * v.cs];
+    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_INVERT) val = T(1) / val;
+    return val;
+  }
+  return x[r * v.rs + c * v.cs];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long mn_len,
+                                                   long k_len, long kk0, long kk1, PackOut o,
+                                                   bool mn_fast_load) {
+  __shared__ T tile[32][33];  // [kk_local][mn_local]
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const long mn_base = (long)blockIdx.x * 32;
+  const long kk_base = kk0 + (long)blockIdx.y * 32;
+
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int a = tx, b = ty + 8 * q;
+    int mn_l = mn_fast_load ? a : b;
+    int kk_l = mn_fast_load ? b : a;
+    long mn = mn_base + mn_l, kk = kk_base + kk_l, kl = kk - kk0;
+    T val = T(0);
+    if (mn < mn_len && kl < k_len && kk < kk1) {
+      long r = b_side ? kl : mn, c = b_side ? mn : kl;
+      val = load_logical<T>(v, r, c);
+    }
+    tile[kk_l][mn_l] = val;
+  }
+  __syncthreads();
+
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int a = tx, b = ty + 8 * q;
+    int mn_l = o.layout == PACK_MN_MAJOR ? a : b;
+    int kk_l = o.layout == PACK_MN_MAJOR ? b : a;
+    long mn = mn_base + mn_l, kk = kk_base + kk_l;
+    if (kk >= kk1) continue;
+    T val = tile[kk_l][mn_l];
+    long off = o.layout == PACK_MN_MAJOR ? kk * o.ld + mn : mn * o.ld + kk;
+    if (o.xform == PACK_COPY) {
+      ((T *)o.out)[off] = val;
+    } else {
+      __nv_bfloat16 *out = (__nv_bfloat16 *)o.out;
+      float f = (float)val;
+      __nv_bfloat16 hi = __float2bfloat16_rn(f);
+      float r1 = f - __bfloat162float(hi);
+      __nv_bfloat16 lo = __float2bfloat16_rn(r1);
+      out[off] = hi;
+      out[off + o.plane_stride] = lo;
+      if (o.terms > 2) {
+        float r2 = r1 - __bfloat162float(lo);
+        out[off + 2 * o.plane_stride] = __float2bfloat16_rn(r2);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn_pad, long kk0,
+                long kk1, const PackOut &o, cudaStream_t s) {
+  if (mn_pad <= 0 || kk1 <= kk0) return B200_OK;
+  long mn_stride = b_side ? v.cs : v.rs;
+  long kk_stride = b_side ? v.rs : v.cs;
+  bool mn_fast = labs(mn_stride) <= labs(kk_stride);
+  dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 32));
+  if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
+  B200ProfScope prof("pack", s);
+  pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, kk0, kk1, o, mn_fast);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
+template int launch_pack<float>(const PackView &, bool, long, long, long, long, long,
+                                const PackOut &, cudaStream_t);
+template int launch_pack<double>(const PackView &, bool, long, long, long, long, long,
+                                 const PackOut &, cudaStream_t);

@@ -1,0 +1,314 @@
+// runtime.cu -- device bring-up, per-thread streams, stream-ordered scratch,
+// strided host<->device staging, error strings, default precision forms and
+// the per-kernel event profiler of libmublis.
+//
+// The reference has no device; its runtime pieces are the pthread_once
+// context (frame/base/safe_dispatch.c:6,64) and the mutex-guarded block pool
+// (frame/base/pool.c:23-66,233-318).  Here the once-init brings up the CUDA
+// device, and the pool is CUDA's stream-ordered allocator (cudaMallocAsync on
+// the calling thread's stream, with the pool's release threshold raised so
+// freed blocks stay cached for the next call).
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "../../include/mublis_b200.h"
+
+namespace {
+
+std::once_flag g_init_once;
+int g_init_status = B200_ECUDA;
+int g_device = 0;
+std::atomic<unsigned long long> g_launches{0};
+
+int g_default_form[2] = {B200_FORM_PLAIN, B200_FORM_PLAIN};
+int g_default_slices = 0;
+
+thread_local cudaStream_t t_stream = nullptr;
+thread_local bool t_stream_owned = false;
+thread_local char t_error[512] = "";
+
+struct ProfRec {
+  const char *name;
+  cudaEvent_t start, stop;
+};
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_prof;
+std::atomic<int> g_prof_on{0};
+
+int parse_form(const char *s, int *slices) {
+  if (!s || !*s) return B200_FORM_AUTO;
+  if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
+  if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
+  if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
+  if (!strncmp(s, "ozaki", 5)) {
+    if (s[5] == ':' && slices) *slices = atoi(s + 6);
+    return B200_FORM_OZAKI;
+  }
+  return B200_FORM_AUTO;
+}
+
+void do_init() {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    snprintf(t_error, sizeof t_error, "no CUDA device: %s",
+             e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+    g_init_status = B200_ECUDA;
+    return;
+  }
+  cudaGetDevice(&g_device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, g_device) != cudaSuccess || prop.major != 10) {
+    snprintf(t_error, sizeof t_error,
+             "libmublis is built for sm_100a (B200); device %d is sm_%d%d", g_device,
+             prop.major, prop.minor);
+    g_init_status = B200_ECUDA;
+    return;
+  }
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, g_device) == cudaSuccess) {
+    uint64_t threshold = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  int slices = 0;
+  int sf = parse_form(getenv("MUBLIS_B200_SFORM"), nullptr);
+  int df = parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
+  if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6)
+    g_default_form[B200_F32] = sf;
+  if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI) g_default_form[B200_F64] = df;
+  if (slices > 0) g_default_slices = slices;
+  g_init_status = B200_OK;
+}
+
+}  // namespace
+
+void b200_note_cuda_error(cudaError_t err, const char *what, const char *file, int line) {
+  snprintf(t_error, sizeof t_error, "%s:%d: %s -> %s", file, line, what,
+           cudaGetErrorString(err));
+  if (getenv("MUBLIS_B200_VERBOSE")) fprintf(stderr, "libmublis: %s\n", t_error);
+}
+
+B200ProfScope::B200ProfScope(const char *name, cudaStream_t s) : slot(-1), stream(s) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!g_prof_on.load(std::memory_order_relaxed)) return;
+  ProfRec r{name, nullptr, nullptr};
+  cudaEventCreate(&r.start);
+  cudaEventCreate(&r.stop);
+  cudaEventRecord(r.start, s);
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  slot = (int)g_prof.size();
+  g_prof.push_back(r);
+}
+
+B200ProfScope::~B200ProfScope() {
+  if (slot < 0) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  cudaEventRecord(g_prof[slot].stop, stream);
+}
+
+extern "C" {
+
+int b200_init(void) {
+  std::call_once(g_init_once, do_init);
+  if (g_init_status != B200_OK && !t_error[0])
+    snprintf(t_error, sizeof t_error, "CUDA device unavailable");
+  return g_init_status;
+}
+
+int b200_device_count(void) {
+  int c = 0;
+  return cudaGetDeviceCount(&c) == cudaSuccess ? c : 0;
+}
+
+int b200_is_device_ptr(const void *p) {
+  if (!p) return 0;
+  cudaPointerAttributes attr;
+  cudaError_t e = cudaPointerGetAttributes(&attr, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void *b200_stream(void) {
+  if (!t_stream) {
+    cudaStreamCreateWithFlags(&t_stream, cudaStreamNonBlocking);
+    t_stream_owned = true;
+  }
+  return (void *)t_stream;
+}
+
+int b200_set_thread_stream(void *stream) {
+  if (t_stream && t_stream_owned) cudaStreamDestroy(t_stream);
+  t_stream = (cudaStream_t)stream;
+  t_stream_owned = false;
+  return B200_OK;
+}
+
+int b200_stream_sync(void) {
+  B200_CUDA_TRY(cudaStreamSynchronize(b200_cur_stream()));
+  return B200_OK;
+}
+
+int b200_alloc(void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 256;
+  B200_CUDA_TRY(cudaMallocAsync(p, bytes, b200_cur_stream()));
+  return B200_OK;
+}
+
+void b200_free(void *p) {
+  if (p) cudaFreeAsync(p, b200_cur_stream());
+}
+
+int b200_set_error(int code, const char *where) {
+  snprintf(t_error, sizeof t_error, "%s", where);
+  return code;
+}
+
+const char *b200_last_error(void) { return t_error; }
+
+int b200_get_default_form(int dtype) { return g_default_form[dtype == B200_F64]; }
+int b200_get_default_slices(void) { return g_default_slices; }
+
+int b200_set_default_form(int dtype, int form, int slices) {
+  if (dtype == B200_F32 && form != B200_FORM_PLAIN && form != B200_FORM_BF16X3 &&
+      form != B200_FORM_BF16X6)
+    return B200_EINVAL;
+  if (dtype == B200_F64 && form != B200_FORM_PLAIN && form != B200_FORM_OZAKI)
+    return B200_EINVAL;
+  g_default_form[dtype == B200_F64] = form;
+  if (slices > 0) g_default_slices = slices;
+  return B200_OK;
+}
+
+// Host -> compact device (column-major rows x cols, leading dimension ld).
+int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long rows, long cols,
+                  size_t elt) {
+  if (rows <= 0 || cols <= 0) return B200_OK;
+  cudaStream_t s = b200_cur_stream();
+  if (rs == 1 && (cols == 1 || cs >= rows)) {
+    B200_CUDA_TRY(cudaMemcpy2DAsync(dst, ld * elt, src, (cols == 1 ? rows : cs) * elt,
+                                    rows * elt, cols, cudaMemcpyHostToDevice, s));
+    return B200_OK;
+  }
+  // General strides: gather on the host into a contiguous staging block.
+  size_t bytes = (size_t)rows * cols * elt;
+  char *stage = (char *)malloc(bytes);
+  if (!stage) return b200_set_error(B200_ENOMEM, "host staging allocation failed");
+  const char *s8 = (const char *)src;
+  for (long j = 0; j < cols; ++j)
+    for (long i = 0; i < rows; ++i)
+      memcpy(stage + (i + j * rows) * elt, s8 + (i * rs + j * cs) * (long)elt, elt);
+  cudaError_t e = cudaMemcpy2DAsync(dst, ld * elt, stage, rows * elt, rows * elt, cols,
+                                    cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  free(stage);
+  B200_CUDA_TRY(e);
+  return B200_OK;
+}
+
+int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,
+                  size_t elt) {
+  if (rows <= 0 || cols <= 0) return B200_OK;
+  cudaStream_t s = b200_cur_stream();
+  if (rs == 1 && (cols == 1 || cs >= rows)) {
+    B200_CUDA_TRY(cudaMemcpy2DAsync(dst, (cols == 1 ? rows : cs) * elt, src, ld * elt,
+                                    rows * elt, cols, cudaMemcpyDeviceToHost, s));
+    return B200_OK;
+  }
+  size_t bytes = (size_t)rows * cols * elt;
+  char *stage = (char *)malloc(bytes);
+  if (!stage) return b200_set_error(B200_ENOMEM, "host staging allocation failed");
+  cudaError_t e = cudaMemcpy2DAsync(stage, rows * elt, src, ld * elt, rows * elt, cols,
+                                    cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    char *d8 = (char *)dst;
+    for (long j = 0; j < cols; ++j)
+      for (long i = 0; i < rows; ++i)
+        memcpy(d8 + (i * rs + j * cs) * (long)elt, stage + (i + j * rows) * elt, elt);
+  }
+  free(stage);
+  B200_CUDA_TRY(e);
+  return B200_OK;
+}
+
+// ---- public runtime controls (include/mublis_b200.h) ----------------------
+
+int mublis_b200_init(void) { return b200_init(); }
+
+const char *mublis_b200_last_error(void) { return b200_last_error(); }
+
+int mublis_b200_set_stream(void *stream) {
+  B200_TRY(b200_init());
+  return b200_set_thread_stream(stream);
+}
+
+void *mublis_b200_get_stream(void) {
+  if (b200_init() != B200_OK) return nullptr;
+  return b200_stream();
+}
+
+int mublis_b200_set_form(char dtype, const char *form) {
+  B200_TRY(b200_init());
+  int slices = 0;
+  int f = parse_form(form, &slices);
+  if (f == B200_FORM_AUTO) return B200_EINVAL;
+  return b200_set_default_form(dtype == 'd' ? B200_F64 : B200_F32, f, slices);
+}
+
+unsigned long long mublis_b200_launch_count(void) { return g_launches.load(); }
+
+int mublis_b200_profile_enable(int on) {
+  g_prof_on.store(on ? 1 : 0);
+  return B200_OK;
+}
+
+// Writes {"kernel": [launches, total_ms], ...} for every launch recorded
+// since the last read, then forgets them.  Synchronises the device.
+int mublis_b200_profile_read(char *buf, unsigned long len) {
+  cudaDeviceSynchronize();
+  std::vector<ProfRec> recs;
+  {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    recs.swap(g_prof);
+  }
+  std::vector<std::pair<std::string, std::pair<int, double>>> agg;
+  for (auto &r : recs) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.start, r.stop);
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+    bool found = false;
+    for (auto &a : agg)
+      if (a.first == r.name) {
+        a.second.first += 1;
+        a.second.second += ms;
+        found = true;
+      }
+    if (!found) agg.push_back({r.name, {1, (double)ms}});
+  }
+  std::string out = "{";
+  for (size_t i = 0; i < agg.size(); ++i) {
+    char tmp[256];
+    snprintf(tmp, sizeof tmp, "%s\"%s\": [%d, %.6f]", i ? ", " : "", agg[i].first.c_str(),
+             agg[i].second.first, agg[i].second.second);
+    out += tmp;
+  }
+  out += "}";
+  if (buf && len) {
+    strncpy(buf, out.c_str(), len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)out.size();
+}
+
+}  // extern "C"
