@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Level-3 BLAS (one JSON line on rank 0).
+
+Workload (N = 1): the plain Level-3 family at n = 4096 in FP32 and FP64 --
+GEMM in all four transA/transB combinations at m = n = k = 4096, SYMM
+left/lower (lower triangle stored), SYRK and SYR2K lower (n = k = 4096),
+TRMM left/lower/non-unit, TRSM left/lower/non-unit (A: off-diagonals
+uniform[-1,1)/n, diagonal uniform[1,2)), B 4096 x 4096, alpha 0.75,
+beta 0.25, column-major, seeded Philox uniform[-1,1) inputs.  One step is
+those 18 calls through the cblas_* entry points.
+
+* value: TFLOP/s of the whole step with operands resident in HBM (device
+  pointers), timed with CUDA events on the library's stream (the caller's
+  torch stream, set with mublis_b200_set_stream).  BLAS flop counts: GEMM
+  2mnk, SYMM 2m^2n, SYRK n(n+1)k, SYR2K 2n(n+1)k, TRMM/TRSM m^2n.
+* e2e: the same step through cblas_* with pinned HOST buffers, so every call
+  stages its operands to the device and its result back inside the timed
+  region.
+* roofline: the dominant kernel's achieved rate from per-launch CUDA events
+  (library profiler, recorded on the launching stream during the timed
+  region) against its pipe's peak.
+* cpu_baseline: the reference's own avx2 build (oracle/_ref) on the host
+  cores, run on a bounded sample (the same family at n = 2048, one pass
+  per host thread, all threads concurrently).
+* --impl reference: the reference's avx2 build timed on the same family
+  (n = 1024 per step, every host thread a concurrent caller).
+
+Multi-GPU: the path does not shard (one BLAS call per GPU); --gpus N runs N
+independent replicas under torchrun, value = total flops / max-over-ranks
+time, scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SGEMM/DGEMM/TRSM TFLOP/s (% of peak) at stated err; served p50/p99 vs plain"
+ROUTINES = ["gemm_nn", "gemm_nt", "gemm_tn", "gemm_tt", "symm", "syrk", "syr2k", "trmm", "trsm"]
+COL, NT, TR, UPPER, LOWER, NONUNIT, LEFT = 102, 111, 112, 121, 122, 131, 141
+ALPHA, BETA = 0.75, 0.25
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # SMs x FP64 FMA lanes x 2 x max clock
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs x FP32 FMA lanes x 2 x max clock
+LEAF = 32  # TRSM diagonal-block leaf size (rows) of the device solve
+
+
+def flops(routine: str, n: int) -> float:
+    if routine.startswith("gemm"):
+        return 2.0 * n ** 3
+    if routine == "symm":
+        return 2.0 * n ** 3
+    if routine == "syrk":
+        return float(n) * (n + 1) * n
+    if routine == "syr2k":
+        return 2.0 * n * (n + 1) * n
+    return float(n) ** 3
+
+
+def family_flops(n: int) -> float:
+    return 2 * sum(flops(r, n) for r in ROUTINES)
+
+
+def kernel_flops(n: int) -> dict:
+    """Flops of one step attributed to the kernel that executes them."""
+    gemm_part = sum(flops(r, n) for r in ROUTINES if r != "trsm") + (n ** 3 - LEAF * n * n)
+    return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part,
+            "trsm_leaf_s": float(LEAF * n * n), "trsm_leaf_d": float(LEAF * n * n)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            pass
+    return {}
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary
+    (profiles/<kernel>_*.txt, line 'dram_bytes_per_launch: N'), or None."""
+    for f in sorted((ROOT / "profiles").glob(f"{kernel}_*.txt")):
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.out = []
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            text, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            text, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in text.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def ref_bench(n: int, threads: int, reps: int, warmup: int) -> dict:
+    from oracle import oracle as orc  # checker/baseline only
+    lib = orc.ref_lib_path("avx2")
+    if not lib.is_file() or not orc.REF_BENCH.is_file():
+        raise FileNotFoundError("reference build missing (make -C oracle)")
+    out = subprocess.run([str(orc.REF_BENCH), str(lib), "family", "x", str(n), str(n), str(n),
+                          str(threads), str(reps), str(warmup)], check=True,
+                         capture_output=True, text=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    n = 1024
+    threads = host_threads()
+    config = workload_config(args.n)
+    try:
+        r = ref_bench(n, threads, args.steps, args.warmup)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build not runnable: {e}"}))
+        return
+    ms = r["wall_s"] / args.steps * 1e3
+    value = r["gflops_aggregate"] / 1e3
+    sample = (f"per step: the 18-call family at m=n=k={n} issued by each of {threads} host "
+              f"threads concurrently (reference linux_avx2 build, 1 thread per call)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic", "config": config,
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def workload_config(n: int) -> dict:
+    return {"workload": f"plain L3 family n={n}: FP32+FP64 GEMM NN/NT/TN/TT, SYMM L/lower, "
+                        f"SYRK lower, SYR2K lower, TRMM L/lower/non-unit, TRSM L/lower/non-unit",
+            "n": n, "calls_per_step": 18, "alpha": ALPHA, "beta": BETA,
+            "layout": "column-major", "forms": {"s": "plain", "d": "plain"},
+            "l2": "inputs larger than L2: every call owns its operands, 4.6 GB per step "
+                  "vs 126 MB L2, so each call starts cold",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------- device arm
+
+class Family:
+    """The 18 calls of one step with their own operands."""
+
+    def __init__(self, torch, lib, n: int, device: bool):
+        self.torch, self.lib, self.n = torch, lib, n
+        self.calls = []
+        self.h2d = 0
+        self.d2h = 0
+        for p, dt in (("s", torch.float32), ("d", torch.float64)):
+            fill = getattr(lib, f"mublis_b200_fill_{p}")
+            elt = 4 if p == "s" else 8
+            for r in ROUTINES:
+                mid = len(self.calls) * 3
+
+                def mat(i, kind=0):
+                    t = torch.empty(n, n, dtype=dt, device="cuda")
+                    assert fill(ctypes.c_void_p(t.data_ptr()), n, n, n, 0, mid + i, kind) == 0
+                    return t
+                a = mat(0)
+                if r in ("trmm", "trsm"):
+                    d = mat(0, 2)
+                    a.div_(n)
+                    a.diagonal().copy_(d.diagonal())
+                    del d
+                b = mat(1)
+                c = mat(2) if r not in ("trmm", "trsm") else None
+                ops = [a, b] + ([c] if c is not None else [])
+                if not device:
+                    ops = [x.cpu().pin_memory() for x in ops]
+                self.calls.append((p, r, ops))
+                n2 = n * n * elt
+                if r in ("trmm", "trsm"):
+                    self.h2d += 2 * n2
+                    self.d2h += n2
+                else:
+                    self.h2d += (2 if r == "syrk" else 3) * n2
+                    self.d2h += n2
+        torch.cuda.synchronize()
+
+    def step(self):
+        lib, n = self.lib, self.n
+        for p, r, ops in self.calls:
+            ptr = [ctypes.c_void_p(x.data_ptr()) for x in ops]
+            if r.startswith("gemm"):
+                ta = TR if r[5] == "t" else NT
+                tb = TR if r[6] == "t" else NT
+                getattr(lib, f"cblas_{p}gemm")(COL, ta, tb, n, n, n, ALPHA, ptr[0], n, ptr[1], n,
+                                               BETA, ptr[2], n)
+            elif r == "symm":
+                getattr(lib, f"cblas_{p}symm")(COL, LEFT, LOWER, n, n, ALPHA, ptr[0], n, ptr[1],
+                                               n, BETA, ptr[2], n)
+            elif r == "syrk":
+                getattr(lib, f"cblas_{p}syrk")(COL, LOWER, NT, n, n, ALPHA, ptr[0], n, BETA,
+                                               ptr[2], n)
+            elif r == "syr2k":
+                getattr(lib, f"cblas_{p}syr2k")(COL, LOWER, NT, n, n, ALPHA, ptr[0], n, ptr[1],
+                                                n, BETA, ptr[2], n)
+            else:
+                getattr(lib, f"cblas_{p}{r}")(COL, LEFT, LOWER, NT, NONUNIT, n, n, ALPHA, ptr[0],
+                                              n, ptr[1], n)
+
+
+def timed(torch, fn, steps: int):
+    s = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def forms_study(torch, lib) -> dict:
+    """Precision forms at m = n = k = 8192 (one call each, event-timed)."""
+    out = {}
+    n = 8192
+    for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6"]),
+                         ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8"])):
+        fill = getattr(lib, f"mublis_b200_fill_{p}")
+        a, b, c = (torch.empty(n, n, dtype=dt, device="cuda") for _ in range(3))
+        for i, x in enumerate((a, b, c)):
+            fill(ctypes.c_void_p(x.data_ptr()), n, n, n, 0, i, 0)
+        fn = getattr(lib, f"cblas_{p}gemm")
+        for f in forms:
+            lib.mublis_b200_set_form(p.encode(), f.encode())
+            call = lambda: fn(COL, NT, NT, n, n, n, 1.0, ctypes.c_void_p(a.data_ptr()), n,  # noqa: E731
+                              ctypes.c_void_p(b.data_ptr()), n, 0.5,
+                              ctypes.c_void_p(c.data_ptr()), n)
+            call()
+            ms = timed(torch, call, 2)
+            out[f"{p}gemm_8192_{f}"] = round(2.0 * n ** 3 / ms / 1e9, 2)
+        lib.mublis_b200_set_form(p.encode(), b"plain")
+        del a, b, c
+        torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mublis", choices=["mublis", "reference"])
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--no-forms", action="store_true", help="skip the 8192 precision-form study")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--only-timed", action="store_true",
+                    help="warm-up + timed steps only (for profiler launch lists)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import mublis_b200 as mb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    lib = mb.load()
+    mb.check(lib.mublis_b200_init(), lib)
+    for p in (b"s", b"d"):
+        lib.mublis_b200_set_form(p, b"plain")
+    stream = torch.cuda.current_stream()
+    mb.check(lib.mublis_b200_set_stream(ctypes.c_void_p(stream.cuda_stream)), lib)
+
+    n = args.n
+    fam = Family(torch, lib, n, device=True)
+    for _ in range(args.warmup):
+        fam.step()
+    torch.cuda.synchronize()
+
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else local
+    sampler = ClockSampler(gpu_index)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    launches0 = lib.mublis_b200_launch_count()
+    lib.mublis_b200_profile_enable(1)
+    ms = timed(torch, fam.step, args.steps)
+    lib.mublis_b200_profile_enable(0)
+    launches = lib.mublis_b200_launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    buf = ctypes.create_string_buffer(1 << 16)
+    lib.mublis_b200_profile_read(buf, len(buf))
+    kstats = json.loads(buf.value.decode() or "{}")
+
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * family_flops(n) / (ms * 1e-3) / 1e12
+
+    # per-routine breakdown (untimed by the headline; one pass, event per call)
+    if args.only_timed:
+        args.no_forms = args.no_cpu = True
+    breakdown = {}
+    if rank == 0 and not args.only_timed:
+        for (p, r, ops), _ in zip(fam.calls, range(len(fam.calls))):
+            single = Family.__new__(Family)
+            single.lib, single.n, single.calls = lib, n, [(p, r, ops)]
+            t1 = timed(torch, single.step, 1)
+            breakdown[f"{p}{r}"] = round(flops(r, n) / (t1 * 1e-3) / 1e12, 2)
+
+    # roofline of the dominant kernel
+    roof = None
+    if kstats and rank == 0:
+        dom = max(kstats, key=lambda k: kstats[k][1])
+        launches_k, total_ms = kstats[dom]
+        kf = kernel_flops(n).get(dom)
+        peaks = measured_peaks()
+        if kf is not None:
+            per_launch = kf * args.steps / launches_k
+            avg_ms = total_ms / launches_k
+            achieved = per_launch / (avg_ms * 1e-3) / 1e12
+            is64 = dom.endswith("d") or "dgemm" in dom
+            peak = FP64_NOMINAL_TFLOPS if is64 else FP32_NOMINAL_TFLOPS
+            traffic = profile_traffic(dom)
+            roof = {"kernel": dom, "bound": "fp64_fma_pipe" if is64 else "fp32_fma_pipe",
+                    "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
+                    "frac": round(achieved / peak, 4),
+                    "peak_source": "nominal (no FMA-pipe peak in MEASURED_PEAKS.json): 148 SMs x "
+                                   + ("64 FP64" if is64 else "128 FP32")
+                                   + " FMA lanes x 2 x 1965 MHz",
+                    "traffic": traffic, "launches_per_step": launches_k / args.steps,
+                    "share_of_step": round(total_ms / args.steps / ms, 4),
+                    "bf16_tflops_measured": peaks.get("bf16_tflops"),
+                    "hbm_gbs_measured": peaks.get("hbm_gbs")}
+
+    # end to end through cblas_* with pinned host buffers
+    e2e = None
+    if not args.only_timed:
+        del fam
+        torch.cuda.empty_cache()
+        hfam = Family(torch, lib, n, device=False)
+        hfam.step()
+        e2e_ms = timed(torch, hfam.step, max(2, min(args.steps, 3)))
+        e2e = {"value": round(family_flops(n) / (e2e_ms * 1e-3) / 1e12, 3), "unit": "TFLOP/s",
+               "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": hfam.h2d,
+               "d2h_bytes_per_step": hfam.d2h, "api": "cblas_* with pinned host buffers"}
+        del hfam
+
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = forms_study(torch, lib)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            threads = host_threads()
+            r = ref_bench(2048, threads, 1, 0)
+            cpu = {"value": round(r["gflops_aggregate"] / 1e3, 4), "unit": "TFLOP/s",
+                   "cores": threads, "kind": "reference",
+                   "sample": f"the 18-call family at m=n=k=2048, one pass per host thread, "
+                             f"{threads} threads concurrently, reference linux_avx2 build "
+                             f"(oracle/_ref), wall {r['wall_s']:.1f} s"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unavailable": str(e)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64", "data": "synthetic: seeded Philox uniform[-1,1); TRSM/TRMM "
+                "A off-diagonal uniform/n, diagonal uniform[1,2)",
+                "config": workload_config(n), "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clocks, "gpu_launches": int(launches), "breakdown_tflops": breakdown,
+                "stated_err": "normwise relative error <= 4*k*u against the oracle "
+                              "(tests/test_gpu_parity.py); measured plain SGEMM ~1.9e-8, "
+                              "DGEMM ~3.4e-17 at 8192 (profiles/precision_forms_8192.md)",
+                "forms_8192_tflops": forms,
+                "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in kstats.items()}}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -95,6 +95,10 @@ int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long ro
 int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,
                   size_t elt);
 
+/* tc_gemm.cu: nonzero (and cleared) if a kernel reported a bounded-wait
+ * timeout since the last call. */
+int b200_take_device_error(void);
+
 /* l3.cu */
 int b200_l3_run(const b200_l3_desc_t *d);
 int b200_trsm_run(const b200_trsm_desc_t *d);

@@ -26,16 +26,33 @@ enum PackLayout {
 };
 
 enum PackXform {
-  PACK_COPY = 0,       // T -> T
-  PACK_BF16_SPLIT = 1  // f32 -> `terms` bf16 planes (hi, lo[, lo2])
+  PACK_COPY = 0,        // T -> T
+  PACK_BF16_SPLIT = 1,  // f32 -> `terms` bf16 planes (hi, lo[, lo2])
+  PACK_INT8_SLICES = 2  // f64 -> `terms` int8 planes of 7-bit slices of
+                        // x * 2^(7 - e), e from the row/column abs-max
 };
 
 struct PackOut {
   void *out;
   long ld;
-  long plane_stride;  // elements between bf16 planes
+  long plane_stride;  // elements between planes
   int layout, xform, terms;
+  const unsigned long long *absmax;  // PACK_INT8_SLICES: bits of max |x| per mn
 };
+
+// Bits of max |x| over kk for every mn of a logical operand view (the
+// Ozaki split's per-row / per-column scale), atomically max-merged into
+// absmax[mn] (which must start at 0).
+int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
+                  unsigned long long *absmax, cudaStream_t s);
+
+// Exponent e with max|x| < 2^e (frexp), 0 for an all-zero row.
+__device__ inline int b200_scale_exp(unsigned long long absmax_bits) {
+  if (absmax_bits == 0) return 0;
+  int e;
+  frexp(__longlong_as_double((long long)absmax_bits), &e);
+  return e;
+}
 
 template <typename T>
 int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn_pad,

@@ -52,8 +52,8 @@ int run_plain(const b200_l3_desc_t *d) {
   B200_TRY(b200_alloc(&ap, sizeof(T) * mpad * kpad));
   int st = b200_alloc(&bp, sizeof(T) * npad * kpad);
   if (st == B200_OK) {
-    PackOut oa{ap, mpad, 0, PACK_MN_MAJOR, PACK_COPY, 1};
-    PackOut ob{bp, npad, 0, PACK_MN_MAJOR, PACK_COPY, 1};
+    PackOut oa{ap, mpad, 0, PACK_MN_MAJOR, PACK_COPY, 1, nullptr};
+    PackOut ob{bp, npad, 0, PACK_MN_MAJOR, PACK_COPY, 1, nullptr};
     st = pack_pairs<T>(d, oa, mpad, ob, npad, kpad, s);
   }
   if (st == B200_OK) {

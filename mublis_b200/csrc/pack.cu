@@ -74,6 +74,16 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
     long off = o.layout == PACK_MN_MAJOR ? kk * o.ld + mn : mn * o.ld + kk;
     if (o.xform == PACK_COPY) {
       ((T *)o.out)[off] = val;
+    } else if (o.xform == PACK_INT8_SLICES) {
+      // Error-free 7-bit slicing (truncation keeps every slice in [-127, 127]):
+      // r = x * 2^(7 - e) in (-128, 128); q_t = trunc(r); r = (r - q_t) * 128.
+      int8_t *out = (int8_t *)o.out;
+      double r = ldexp((double)val, 7 - b200_scale_exp(o.absmax[mn]));
+      for (int t = 0; t < o.terms; ++t) {
+        double q = trunc(r);
+        out[off + t * o.plane_stride] = (int8_t)(int)q;
+        r = (r - q) * 128.0;
+      }
     } else {
       __nv_bfloat16 *out = (__nv_bfloat16 *)o.out;
       float f = (float)val;
@@ -90,7 +100,51 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) absmax_kernel(PackView v, bool b_side, long mn_len,
+                                                     long k_len, bool mn_fast_load,
+                                                     unsigned long long *absmax) {
+  __shared__ double tile[32][33];  // [kk_local][mn_local]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const long mn_base = (long)blockIdx.x * 32, kk_base = (long)blockIdx.y * 32;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int a = tx, b = ty + 8 * q;
+    int mn_l = mn_fast_load ? a : b, kk_l = mn_fast_load ? b : a;
+    long mn = mn_base + mn_l, kk = kk_base + kk_l;
+    double val = 0.0;
+    if (mn < mn_len && kk < k_len) {
+      long r = b_side ? kk : mn, c = b_side ? mn : kk;
+      val = fabs((double)load_logical<T>(v, r, c));
+    }
+    tile[kk_l][mn_l] = val;
+  }
+  __syncthreads();
+  if (ty == 0) {
+    double mx = 0.0;
+#pragma unroll 8
+    for (int kk = 0; kk < 32; ++kk) mx = fmax(mx, tile[kk][tx]);
+    long mn = mn_base + tx;
+    if (mn < mn_len && mx > 0.0)
+      atomicMax(&absmax[mn], (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
 }  // namespace
+
+int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
+                  unsigned long long *absmax, cudaStream_t s) {
+  if (mn_len <= 0 || k_len <= 0) return B200_OK;
+  long mn_stride = b_side ? v.cs : v.rs;
+  long kk_stride = b_side ? v.rs : v.cs;
+  bool mn_fast = labs(mn_stride) <= labs(kk_stride);
+  dim3 grid((unsigned)b200_ceil_div(mn_len, 32), (unsigned)b200_ceil_div(k_len, 32));
+  if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
+  B200ProfScope prof("absmax", s);
+  absmax_kernel<double><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, mn_fast, absmax);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
 
 template <typename T>
 int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn_pad, long kk0,

@@ -154,6 +154,8 @@ int b200_set_thread_stream(void *stream) {
 
 int b200_stream_sync(void) {
   B200_CUDA_TRY(cudaStreamSynchronize(b200_cur_stream()));
+  if (int e = b200_take_device_error())
+    return b200_set_error(e, "a device-side bounded wait timed out (kernel aborted)");
   return B200_OK;
 }
 

@@ -1,9 +1,776 @@
-// tc_gemm.cu -- tcgen05 contraction forms (placeholder until the kernels land).
+// tc_gemm.cu -- tcgen05 forms of the L3 contraction.
+//
+// BF16x3 / BF16x6 (FP32-class):  every FP32 operand element x is split in
+// the pack pass into bf16 terms x = h + l (+ l2); the kernel accumulates in
+// one FP32 TMEM accumulator the products whose term indices sum to < TERMS
+// (hi*hi + hi*lo + lo*hi for x3; plus hi*lo2 + lo*lo + lo2*hi for x6).
+//
+// Kernel shape (sm_100a, one CTA per SM, persistent over output tiles):
+//   warp 0      TMA producer: per k-block, TERMS A-plane tiles (128 x 32 bf16)
+//               and TERMS B-plane tiles (256 x 32 bf16), 64-byte swizzle,
+//               into a STAGES-deep ring guarded by full/empty mbarriers
+//   warp 1      MMA issuer: one thread issues tcgen05.mma (M=128, N=256,
+//               K=16) into a TMEM accumulator, commits stage releases
+//   warp 2      allocates / frees 512 TMEM columns: two 256-column window
+//               accumulators, so the MMAs of window w+1 overlap the drain
+//               of window w
+//   warps 4-11  epilogue (two warps per TMEM lane quadrant, 128 columns
+//               each): every FLUSH k-blocks (256 k) a thread folds its row's
+//               window accumulator (tcgen05.ld) into a 128-wide FP32 running
+//               sum held in registers, with round-to-nearest adds; after the
+//               last window it applies alpha/beta, the domain's ji mask and
+//               the m/n edge and stores column-major C with coalesced writes
+// Why windows: the tensor core's FP32 accumulation does not round to
+// nearest, so its error grows with the number of accumulation steps; with
+// a 256-deep window the sum over windows is an ordinary RN FP32 sum and the
+// error matches a scalar FP32 loop.
+// The tile walk, domain pruning and k-range clipping are the same as the
+// plain kernel's (gemm_simt.cu), i.e. the reference driver's
+// (frame/l3/l3_driver.c:130-171); a tile without update writes beta * C.
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <mutex>
+
+#include "kernels.cuh"
+#include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
-int tc_run_bf16(const b200_l3_desc_t *, int) {
-  return b200_set_error(B200_EINVAL, "bf16 split form not available in this build");
+// ---- host helpers ------------------------------------------------------------
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+int *g_err_host = nullptr;
+int *g_err_dev = nullptr;
+std::once_flag g_err_once;
+
+void init_encode() {
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+          cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
 }
-int tc_run_ozaki(const b200_l3_desc_t *) {
-  return b200_set_error(B200_EINVAL, "ozaki form not available in this build");
+
+void init_err() {
+  if (cudaHostAlloc((void **)&g_err_host, sizeof(int), cudaHostAllocMapped) == cudaSuccess) {
+    *g_err_host = 0;
+    cudaHostGetDevicePointer((void **)&g_err_dev, g_err_host, 0);
+  }
+}
+
+}  // namespace
+
+int *b200_device_error_word() {
+  std::call_once(g_err_once, init_err);
+  return g_err_dev;
+}
+
+extern "C" int b200_take_device_error(void) {
+  if (!g_err_host) return 0;
+  int e = *(volatile int *)g_err_host;
+  if (e) *(volatile int *)g_err_host = 0;
+  return e;
+}
+
+int b200_make_tmap(CUtensorMap *map, const void *base, int is_bf16, long k, long rows, int box_k,
+                   int box_rows, int swz) {
+  std::call_once(g_encode_once, init_encode);
+  if (!g_encode) return b200_set_error(B200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  const int elt = is_bf16 ? 2 : 1;
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(k * elt)};
+  cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, is_bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                        2, const_cast<void *>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        swz == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return b200_set_error(B200_ECUDA, "cuTensorMapEncodeTiled failed");
+  return B200_OK;
+}
+
+// ---- shared tile walk ---------------------------------------------------------
+
+namespace {
+
+struct TileWalk {
+  int tiles_m, tiles_n, bm, bn;
+  int m, n, kblocks, bk;
+  long k;
+  int jp, ji, pi;
+
+  __device__ __forceinline__ void coords(int idx, int &tm, int &tn) const {
+    constexpr int G = 8;
+    int group = idx / (G * tiles_n);
+    int first = group * G;
+    int gsize = min(tiles_m - first, G);
+    int in_group = idx % (G * tiles_n);
+    tm = first + in_group % gsize;
+    tn = in_group / gsize;
+  }
+  __device__ __forceinline__ bool valid(int tm, int tn) const {
+    long m0 = (long)tm * bm, n0 = (long)tn * bn;
+    if (ji == MUBLIS_L3_LOWER && n0 >= m0 + bm) return false;
+    if (ji == MUBLIS_L3_UPPER && n0 + bn <= m0) return false;
+    return true;
+  }
+  __device__ __forceinline__ void krange(int tm, int tn, int &kb0, int &kb1) const {
+    long m0 = (long)tm * bm, n0 = (long)tn * bn;
+    long lo = 0, hi = k;
+    if (jp == MUBLIS_L3_LOWER) lo = max(lo, n0);
+    if (jp == MUBLIS_L3_UPPER) hi = min(hi, n0 + bn);
+    if (pi == MUBLIS_L3_LOWER) hi = min(hi, m0 + bm);
+    if (pi == MUBLIS_L3_UPPER) lo = max(lo, m0);
+    kb0 = (int)(lo / bk);
+    kb1 = hi > lo ? (int)((hi + bk - 1) / bk) : kb0;
+  }
+};
+
+struct Bf16Params {
+  TileWalk w;
+  long mpad, npad;  // rows per plane
+  float alpha, beta;
+  float *c;
+  long rs_c, cs_c;
+  int *err;
+};
+
+template <int TERMS, int STAGES>
+struct Bf16Cfg {
+  static constexpr int BM = 128, BN = 256, SWZ = 64, BK = SWZ / 2;
+  static constexpr int A_TILE = BM * SWZ, B_TILE = BN * SWZ;
+  static constexpr int STAGE_BYTES = TERMS * (A_TILE + B_TILE);
+  static constexpr int KSTEPS = SWZ / 32;
+  static constexpr int FLUSH = 8;  // k-blocks (8 x 32 = 256 k) per TMEM window
+  static constexpr int THREADS = 384;
+  static constexpr int EPI_THREADS = 256;
+  static constexpr int HALF = BN / 2;  // columns per epilogue thread
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr uint32_t TMEM_COLS = 512;
+};
+
+template <int TERMS, int STAGES>
+__global__ void __launch_bounds__(384, 1)
+    tc_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   Bf16Params p) {
+  using C = Bf16Cfg<TERMS, STAGES>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      tc::mbar_init(&tfull[a], 1);
+      tc::mbar_init(&tempty[a], C::EPI_THREADS);
+    }
+    tc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    tc::fence_barrier_init();
+    tc::tma_prefetch_desc(&tmA);
+    tc::tma_prefetch_desc(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const TileWalk &w = p.w;
+  const int num_tiles = w.tiles_m * w.tiles_n;
+  auto sa = [&](int s, int t) { return smem + s * C::STAGE_BYTES + t * C::A_TILE; };
+  auto sb = [&](int s, int t) {
+    return smem + s * C::STAGE_BYTES + TERMS * C::A_TILE + t * C::B_TILE;
+  };
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int stage = 0;
+    uint32_t phase = 0;
+    int issued = 0;
+    bool ok = true;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        tc::mbar_arrive_expect_tx(&full[stage], C::STAGE_BYTES);
+#pragma unroll
+        for (int t = 0; t < TERMS; ++t)
+          tc::tma_load_2d(sa(stage, t), &tmA, &full[stage], kb * C::BK,
+                          (int)(t * p.mpad + (long)tm * C::BM));
+#pragma unroll
+        for (int t = 0; t < TERMS; ++t)
+          tc::tma_load_2d(sb(stage, t), &tmB, &full[stage], kb * C::BK,
+                          (int)(t * p.npad + (long)tn * C::BN));
+        ++issued;
+        if (++stage == STAGES) { stage = 0; phase ^= 1; }
+      }
+    }
+    // Drain: wait (bounded) for the loads of the last ring's worth of stages.
+    int pending = issued < STAGES ? issued : STAGES;
+    for (int q = 0; q < pending; ++q) {
+      if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
+      if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) break;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t IDESC = tc::idesc_bf16(C::BM, C::BN);
+    int stage = 0, acc = 0;
+    uint32_t phase = 0, acc_phase = 0;
+    bool ok = true, any = false;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += C::FLUSH) {
+        const int c1 = min(kb1, c0 + C::FLUSH);
+        // The epilogue has drained this window buffer's previous use.
+        if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        tc::tc_fence_after();
+        const uint32_t d = tmem_base + (uint32_t)(acc * C::BN);
+        for (int kb = c0; kb < c1; ++kb) {
+          if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
+          tc::tc_fence_after();
+#pragma unroll
+          for (int ks = 0; ks < C::KSTEPS; ++ks) {
+            // Small terms first, the hi*hi product last.
+#pragma unroll
+            for (int sum = TERMS - 1; sum >= 0; --sum) {
+#pragma unroll
+              for (int ta = 0; ta <= sum; ++ta) {
+                const int tb = sum - ta;
+                uint64_t ad = tc::smem_desc(sa(stage, ta), C::SWZ) + (uint64_t)((ks * 32) >> 4);
+                uint64_t bd = tc::smem_desc(sb(stage, tb), C::SWZ) + (uint64_t)((ks * 32) >> 4);
+                const bool first = kb == c0 && ks == 0 && sum == TERMS - 1 && ta == 0;
+                tc::mma_bf16(d, ad, bd, IDESC, first ? 0u : 1u);
+              }
+            }
+          }
+          tc::mma_commit(&empty[stage]);
+          any = true;
+          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+        tc::mma_commit(&tfull[acc]);
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+      }
+    }
+    if (any) {  // every issued MMA has completed before TMEM is released
+      tc::mma_commit(drain);
+      tc::mbar_wait(drain, 0, abort_flag, p.err);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue ----------------
+    const int quad = warp & 3;        // TMEM lanes 32*quad .. 32*quad+31
+    const int half = (warp - 4) >> 2; // columns [half*128, half*128+128)
+    const int row = quad * 32 + lane;
+    const uint32_t lane_base = tmem_base + ((uint32_t)(quad * 32) << 16);
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    float run[C::HALF];
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const long gi = (long)tm * C::BM + row;
+      const bool row_ok = gi < w.m;
+      const long gj0 = (long)tn * C::BN + half * C::HALF;
+      if (kb0 >= kb1) {  // no update: beta * C
+        if (row_ok)
+          for (int j = 0; j < C::HALF; ++j) {
+            const long gj = gj0 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            float *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+            *cij = p.beta != 0.f ? p.beta * *cij : 0.f;
+          }
+        continue;
+      }
+      const int nwin = (kb1 - kb0 + C::FLUSH - 1) / C::FLUSH;
+      for (int win = 0; win < nwin; ++win) {
+        // Every lane observes the barrier; the outcome is made warp-uniform
+        // because the TMEM loads below are .sync.aligned.
+        int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
+        if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
+        tc::tc_fence_after();
+        const uint32_t base = lane_base + (uint32_t)(acc * C::BN + half * C::HALF);
+#pragma unroll
+        for (int g = 0; g < C::HALF / 16; ++g) {
+          uint32_t r[16];
+          tc::tmem_ld16(base + (uint32_t)(g * 16), r);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            run[g * 16 + j] = win == 0 ? __uint_as_float(r[j])
+                                       : __fadd_rn(run[g * 16 + j], __uint_as_float(r[j]));
+        }
+        tc::tc_fence_before();
+        tc::mbar_arrive(&tempty[acc]);
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+      }
+      if (!ok) break;
+      if (row_ok) {
+#pragma unroll
+        for (int j = 0; j < C::HALF; ++j) {
+          const long gj = gj0 + j;
+          if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+          float *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+          float v = p.alpha * run[j];
+          if (p.beta != 0.f) v = fmaf(p.beta, *cij, v);
+          *cij = v;
+        }
+      }
+    }
+  }
+
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_base, C::TMEM_COLS);
+  }
+}
+
+template <int TERMS, int STAGES>
+int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &p,
+                cudaStream_t s) {
+  using C = Bf16Cfg<TERMS, STAGES>;
+  auto kern = tc_bf16_kernel<TERMS, STAGES>;
+  static bool configured = false;
+  if (!configured) {
+    B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    configured = true;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int tiles = p.w.tiles_m * p.w.tiles_n;
+  int grid = tiles < sms ? tiles : sms;
+  B200ProfScope prof(TERMS == 2 ? "tc_bf16x3" : "tc_bf16x6", s);
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
+}  // namespace
+
+// Packs the FP32 operands into TERMS bf16 planes (K-major, padded) and runs
+// the tcgen05 kernel.
+int tc_run_bf16(const b200_l3_desc_t *d, int form) {
+  if (d->dtype != B200_F32) return b200_set_error(B200_EINVAL, "bf16 forms are FP32-only");
+  const int terms = form == B200_FORM_BF16X6 ? 3 : 2;
+  constexpr int BM = 128, BN = 256, BK = 32;
+  cudaStream_t s = b200_cur_stream();
+  const long ktot = (long)d->k * d->npairs;
+  const long mpad = b200_round_up(d->m, BM), npad = b200_round_up(d->n, BN);
+  const long kpad = b200_round_up(ktot, BK);
+  if (terms * (mpad > npad ? mpad : npad) > 0x7fffffffL)
+    return b200_set_error(B200_EINVAL, "bf16 form: operand too large for 32-bit TMA rows");
+  void *ap = nullptr, *bp = nullptr;
+  B200_TRY(b200_alloc(&ap, sizeof(uint16_t) * terms * mpad * kpad));
+  int st = b200_alloc(&bp, sizeof(uint16_t) * terms * npad * kpad);
+  const mublis_l3_product_t &pr = d->product;
+  for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
+    long kk0 = (long)t * d->k, kk1 = t + 1 == d->npairs ? kpad : kk0 + d->k;
+    PackView va{d->a[t], d->rs_a[t], d->cs_a[t], (int)pr.a.struc, (int)pr.a.uplo,
+                (int)pr.a.diag, (int)pr.domain.pi};
+    PackView vb{d->b[t], d->rs_b[t], d->cs_b[t], (int)pr.b.struc, (int)pr.b.uplo,
+                (int)pr.b.diag, (int)pr.domain.jp};
+    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, PACK_BF16_SPLIT, terms, nullptr};
+    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, PACK_BF16_SPLIT, terms, nullptr};
+    st = launch_pack<float>(va, false, d->m, d->k, mpad, kk0, kk1, oa, s);
+    if (st == B200_OK) st = launch_pack<float>(vb, true, d->n, d->k, npad, kk0, kk1, ob, s);
+  }
+  CUtensorMap ta, tb;
+  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 1, kpad, terms * mpad, BK, BM, 64);
+  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 1, kpad, terms * npad, BK, BN, 64);
+  if (st == B200_OK) {
+    Bf16Params p;
+    p.w.tiles_m = (int)(mpad / BM);
+    p.w.tiles_n = (int)(npad / BN);
+    p.w.bm = BM;
+    p.w.bn = BN;
+    p.w.m = d->m;
+    p.w.n = d->n;
+    p.w.k = ktot;
+    p.w.bk = BK;
+    p.w.kblocks = (int)(kpad / BK);
+    p.w.jp = pr.domain.jp;
+    p.w.ji = pr.domain.ji;
+    p.w.pi = pr.domain.pi;
+    p.mpad = mpad;
+    p.npad = npad;
+    p.alpha = (float)d->alpha;
+    p.beta = (float)d->beta;
+    p.c = (float *)d->c;
+    p.rs_c = d->rs_c;
+    p.cs_c = d->cs_c;
+    p.err = b200_device_error_word();
+    st = terms == 2 ? launch_bf16<2, 4>(ta, tb, p, s) : launch_bf16<3, 3>(ta, tb, p, s);
+  }
+  b200_free(ap);
+  b200_free(bp);
+  return st;
+}
+
+// ---- Ozaki split-integer FP64 ---------------------------------------------------
+//
+// op(A) row i is scaled by 2^-e_i and op(B) column j by 2^-f_j (e, f from the
+// abs-max, so scaled values lie in (-1, 1)), and each scaled value is cut
+// into s signed 7-bit slices: a = 2^e_i sum_t A_t 2^-7t, b = 2^f_j sum_u B_u
+// 2^-7u (pack.cu).  Then C = 2^(e_i + f_j) sum_d 2^-7d S_d with
+// S_d = sum_{t+u=d} A_t B_u, keeping the diagonals d <= s + 1.  Every S_d is
+// an exact int32 tcgen05 (kind::i8) accumulation as long as
+// s * kchunk * 127^2 < 2^31, so k is processed in chunks of 8192 and s <= 12.
+// The epilogue drains S_d from TMEM, adds ldexp(S_d, -7d) in FP64 into a
+// per-CTA tile workspace (L2-resident), and on the last phase writes
+// C = alpha * ldexp(W, e_i + f_j) + beta * C.  Phases (k-chunk, d) run from
+// the smallest d contribution to the largest; two TMEM accumulators let the
+// epilogue of one phase overlap the MMAs of the next.
+
+namespace {
+
+constexpr int OZ_MAX_SLICES = 12;
+constexpr int OZ_KCHUNK_BLOCKS = 64;  // 64 x 128 = 8192 k per exact int32 chunk
+
+struct OzParams {
+  TileWalk w;
+  long mpad, npad;
+  int slices;
+  double alpha, beta;
+  double *c;
+  long rs_c, cs_c;
+  double *work;  // gridDim.x tiles of 128 x 256 doubles
+  const unsigned long long *amax, *bmax;
+  int *err;
+};
+
+struct OzCfg {
+  static constexpr int BM = 128, BN = 256, SWZ = 128, BK = 128, STAGES = 4;
+  static constexpr int A_TILE = BM * SWZ, B_TILE = BN * SWZ;
+  static constexpr int STAGE_BYTES = A_TILE + B_TILE;
+  static constexpr int KSTEPS = SWZ / 32;
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr uint32_t TMEM_COLS = 512;
+};
+
+__global__ void __launch_bounds__(256, 1)
+    tc_ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    OzParams p) {
+  using C = OzCfg;
+  constexpr int STAGES = C::STAGES;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      tc::mbar_init(&tfull[a], 1);
+      tc::mbar_init(&tempty[a], 128);
+    }
+    tc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    tc::fence_barrier_init();
+    tc::tma_prefetch_desc(&tmA);
+    tc::tma_prefetch_desc(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc(tmem_slot, C::TMEM_COLS);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const TileWalk &w = p.w;
+  const int S = p.slices;
+  const int num_tiles = w.tiles_m * w.tiles_n;
+  auto sa = [&](int st) { return smem + st * C::STAGE_BYTES; };
+  auto sb = [&](int st) { return smem + st * C::STAGE_BYTES + C::A_TILE; };
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int stage = 0, issued = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += OZ_KCHUNK_BLOCKS) {
+        const int c1 = min(kb1, c0 + OZ_KCHUNK_BLOCKS);
+        for (int d = S + 1; d >= 2 && ok; --d) {
+          for (int t = max(1, d - S); t <= min(S, d - 1) && ok; ++t) {
+            const int u = d - t;
+            for (int kb = c0; kb < c1; ++kb) {
+              if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+              tc::mbar_arrive_expect_tx(&full[stage], C::STAGE_BYTES);
+              tc::tma_load_2d(sa(stage), &tmA, &full[stage], kb * C::BK,
+                              (int)((t - 1) * p.mpad + (long)tm * C::BM));
+              tc::tma_load_2d(sb(stage), &tmB, &full[stage], kb * C::BK,
+                              (int)((u - 1) * p.npad + (long)tn * C::BN));
+              ++issued;
+              if (++stage == STAGES) { stage = 0; phase ^= 1; }
+            }
+          }
+        }
+      }
+    }
+    int pending = issued < STAGES ? issued : STAGES;
+    for (int q = 0; q < pending; ++q) {
+      if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
+      if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) break;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t IDESC = tc::idesc_s8(C::BM, C::BN);
+    int stage = 0, acc = 0;
+    uint32_t phase = 0, acc_phase = 0;
+    bool ok = true, any = false;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += OZ_KCHUNK_BLOCKS) {
+        const int c1 = min(kb1, c0 + OZ_KCHUNK_BLOCKS);
+        for (int d = S + 1; d >= 2 && ok; --d) {
+          if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+          tc::tc_fence_after();
+          const uint32_t dt = tmem_base + (uint32_t)(acc * C::BN);
+          bool first = true;
+          for (int t = max(1, d - S); t <= min(S, d - 1) && ok; ++t) {
+            for (int kb = c0; kb < c1; ++kb) {
+              if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
+              tc::tc_fence_after();
+              const uint64_t ad = tc::smem_desc(sa(stage), C::SWZ);
+              const uint64_t bd = tc::smem_desc(sb(stage), C::SWZ);
+#pragma unroll
+              for (int ks = 0; ks < C::KSTEPS; ++ks) {
+                tc::mma_i8(dt, ad + (uint64_t)((ks * 32) >> 4), bd + (uint64_t)((ks * 32) >> 4),
+                           IDESC, first ? 0u : 1u);
+                first = false;
+              }
+              tc::mma_commit(&empty[stage]);
+              any = true;
+              if (++stage == STAGES) { stage = 0; phase ^= 1; }
+            }
+          }
+          if (!ok) break;
+          tc::mma_commit(&tfull[acc]);
+          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+      }
+    }
+    if (any) {
+      tc::mma_commit(drain);
+      tc::mbar_wait(drain, 0, abort_flag, p.err);
+    }
+  } else if (warp >= 4) {
+    // ---------------- epilogue ----------------
+    const int ew = warp - 4;
+    const int row = ew * 32 + lane;
+    double *W = p.work + (size_t)blockIdx.x * C::BM * C::BN;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const long gi = (long)tm * C::BM + row;
+      const bool row_ok = gi < w.m;
+      const int ei = row_ok ? b200_scale_exp(p.amax[gi]) : 0;
+      if (kb0 >= kb1) {  // no update: beta * C
+        if (row_ok)
+          for (int j = 0; j < C::BN; ++j) {
+            const long gj = (long)tn * C::BN + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+            *cij = p.beta != 0.0 ? p.beta * *cij : 0.0;
+          }
+        continue;
+      }
+      const int nchunks = (kb1 - kb0 + OZ_KCHUNK_BLOCKS - 1) / OZ_KCHUNK_BLOCKS;
+      const int nph = nchunks * S;
+      int ph = 0;
+      for (int cc = 0; cc < nchunks && ok; ++cc) {
+        for (int d = S + 1; d >= 2; --d, ++ph) {
+          int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
+          if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
+          tc::tc_fence_after();
+          const bool last = ph == nph - 1;
+#pragma unroll 1
+          for (int ch = 0; ch < C::BN / 16; ++ch) {
+            uint32_t r[16];
+            tc::tmem_ld16(tmem_base + ((uint32_t)(ew * 32) << 16) +
+                              (uint32_t)(acc * C::BN + ch * 16), r);
+            tc::tmem_wait_ld();
+            if (!row_ok) continue;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int col = ch * 16 + j;
+              double *wp = W + row + (size_t)col * C::BM;
+              double v = ldexp((double)(int)r[j], -7 * d);
+              if (ph > 0) v += *wp;
+              if (!last) {
+                *wp = v;
+                continue;
+              }
+              const long gj = (long)tn * C::BN + col;
+              if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+              double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+              double out = p.alpha * ldexp(v, ei + b200_scale_exp(p.bmax[gj]));
+              if (p.beta != 0.0) out = fma(p.beta, *cij, out);
+              *cij = out;
+            }
+          }
+          tc::tc_fence_before();
+          tc::mbar_arrive(&tempty[acc]);
+          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+      }
+    }
+  }
+
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_base, C::TMEM_COLS);
+  }
+}
+
+}  // namespace
+
+int tc_run_ozaki(const b200_l3_desc_t *d) {
+  if (d->dtype != B200_F64) return b200_set_error(B200_EINVAL, "ozaki form is FP64-only");
+  using C = OzCfg;
+  int slices = d->slices > 0 ? d->slices : b200_get_default_slices();
+  if (slices <= 0) slices = 7;
+  if (slices < 2 || slices > OZ_MAX_SLICES)
+    return b200_set_error(B200_EINVAL, "ozaki: slice count must be in [2, 12]");
+  cudaStream_t s = b200_cur_stream();
+  const long ktot = (long)d->k * d->npairs;
+  const long mpad = b200_round_up(d->m, C::BM), npad = b200_round_up(d->n, C::BN);
+  const long kpad = b200_round_up(ktot, C::BK);
+  if (slices * (mpad > npad ? mpad : npad) > 0x7fffffffL)
+    return b200_set_error(B200_EINVAL, "ozaki form: operand too large for 32-bit TMA rows");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const int tiles = (int)((mpad / C::BM) * (npad / C::BN));
+  const int grid = tiles < sms ? tiles : sms;
+
+  void *ap = nullptr, *bp = nullptr, *amax = nullptr, *bmax = nullptr, *work = nullptr;
+  int st = b200_alloc(&amax, sizeof(unsigned long long) * (mpad + npad));
+  if (st == B200_OK) {
+    bmax = (unsigned long long *)amax + mpad;
+    st = cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * (mpad + npad), s) == cudaSuccess
+             ? B200_OK
+             : b200_set_error(B200_ECUDA, "memset failed");
+  }
+  if (st == B200_OK) st = b200_alloc(&ap, (size_t)slices * mpad * kpad);
+  if (st == B200_OK) st = b200_alloc(&bp, (size_t)slices * npad * kpad);
+  if (st == B200_OK) st = b200_alloc(&work, sizeof(double) * grid * C::BM * C::BN);
+  const mublis_l3_product_t &pr = d->product;
+  PackView va[2], vb[2];
+  for (int t = 0; t < d->npairs; ++t) {
+    va[t] = PackView{d->a[t], d->rs_a[t], d->cs_a[t], (int)pr.a.struc, (int)pr.a.uplo,
+                     (int)pr.a.diag, (int)pr.domain.pi};
+    vb[t] = PackView{d->b[t], d->rs_b[t], d->cs_b[t], (int)pr.b.struc, (int)pr.b.uplo,
+                     (int)pr.b.diag, (int)pr.domain.jp};
+  }
+  // Scales over the whole (concatenated) k of every row / column.
+  for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
+    st = launch_absmax(va[t], false, d->m, d->k, (unsigned long long *)amax, s);
+    if (st == B200_OK) st = launch_absmax(vb[t], true, d->n, d->k, (unsigned long long *)bmax, s);
+  }
+  for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
+    long kk0 = (long)t * d->k, kk1 = t + 1 == d->npairs ? kpad : kk0 + d->k;
+    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, PACK_INT8_SLICES, slices,
+               (const unsigned long long *)amax};
+    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, PACK_INT8_SLICES, slices,
+               (const unsigned long long *)bmax};
+    st = launch_pack<double>(va[t], false, d->m, d->k, mpad, kk0, kk1, oa, s);
+    if (st == B200_OK) st = launch_pack<double>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
+  }
+  CUtensorMap ta, tb;
+  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 0, kpad, slices * mpad, C::BK, C::BM, 128);
+  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 0, kpad, slices * npad, C::BK, C::BN, 128);
+  if (st == B200_OK) {
+    OzParams p;
+    p.w.tiles_m = (int)(mpad / C::BM);
+    p.w.tiles_n = (int)(npad / C::BN);
+    p.w.bm = C::BM;
+    p.w.bn = C::BN;
+    p.w.m = d->m;
+    p.w.n = d->n;
+    p.w.k = ktot;
+    p.w.bk = C::BK;
+    p.w.kblocks = (int)(kpad / C::BK);
+    p.w.jp = pr.domain.jp;
+    p.w.ji = pr.domain.ji;
+    p.w.pi = pr.domain.pi;
+    p.mpad = mpad;
+    p.npad = npad;
+    p.slices = slices;
+    p.alpha = d->alpha;
+    p.beta = d->beta;
+    p.c = (double *)d->c;
+    p.rs_c = d->rs_c;
+    p.cs_c = d->cs_c;
+    p.work = (double *)work;
+    p.amax = (const unsigned long long *)amax;
+    p.bmax = (const unsigned long long *)bmax;
+    p.err = b200_device_error_word();
+    static bool configured = false;
+    if (!configured) {
+      if (cudaFuncSetAttribute(tc_ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               C::SMEM) != cudaSuccess)
+        st = b200_set_error(B200_ECUDA, "ozaki: smem attribute");
+      configured = st == B200_OK;
+    }
+    if (st == B200_OK) {
+      B200ProfScope prof("tc_ozaki_i8", s);
+      tc_ozaki_kernel<<<grid, 256, C::SMEM, s>>>(ta, tb, p);
+      if (cudaGetLastError() != cudaSuccess) st = b200_set_error(B200_ECUDA, "ozaki launch failed");
+    }
+  }
+  b200_free(ap);
+  b200_free(bp);
+  b200_free(work);
+  b200_free(amax);
+  return st;
 }

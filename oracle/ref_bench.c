@@ -6,8 +6,10 @@
  *   ref_bench LIB ROUTINE DTYPE M N K THREADS REPS WARMUP
  *     ROUTINE  gemm_nn gemm_nt gemm_tn gemm_tt symm syrk syr2k trmm trsm
  *              (symm/trmm/trsm: left, lower, non-unit; syrk/syr2k: lower,
- *              no-trans -- the shapes of the plain-family workload)
- *     DTYPE    s | d
+ *              no-trans -- the shapes of the plain-family workload), or
+ *              "family": all nine in both precisions, one after another
+ *              (m = n = k = M), as one timed unit
+ *     DTYPE    s | d (ignored for "family")
  *
  * Every thread owns its operands (seeded Philox uniform[-1,1), column-major;
  * TRSM's A has off-diagonals uniform/m and a diagonal in [1,2)) and issues
@@ -41,6 +43,8 @@ typedef void (*tr_d_t)(int, int, int, int, int, int, int, double, const double *
 static void *g_lib;
 static const char *g_routine;
 static int g_dbl, g_m, g_n, g_k, g_threads, g_reps, g_warmup;
+static const char *FAMILY[] = {"gemm_nn", "gemm_nt", "gemm_tn", "gemm_tt", "symm",
+                               "syrk",    "syr2k",   "trmm",    "trsm"};
 static pthread_barrier_t g_start, g_done;
 static double *g_times;
 
@@ -56,45 +60,44 @@ static void *sym(const char *name) {
   return f;
 }
 
-static void fill(void *x, long m, long n, uint32_t id, int trsm_a) {
+static void fill(int dbl, void *x, long m, long n, uint32_t id, int trsm_a) {
   for (long j = 0; j < n; ++j)
     for (long i = 0; i < m; ++i) {
       uint64_t idx = (uint64_t)(i + j * m);
       double v;
-      if (trsm_a && i == j) v = g_dbl ? philox_draw_f64(idx, 0, id, PHILOX_DRAW_DIAG)
+      if (trsm_a && i == j) v = dbl ? philox_draw_f64(idx, 0, id, PHILOX_DRAW_DIAG)
                                        : philox_draw_f32(idx, 0, id, PHILOX_DRAW_DIAG);
       else {
-        v = g_dbl ? philox_draw_f64(idx, 0, id, PHILOX_DRAW_UNIFORM)
+        v = dbl ? philox_draw_f64(idx, 0, id, PHILOX_DRAW_UNIFORM)
                   : philox_draw_f32(idx, 0, id, PHILOX_DRAW_UNIFORM);
         if (trsm_a) v /= (double)m;
       }
-      if (g_dbl) ((double *)x)[i + j * m] = v;
+      if (dbl) ((double *)x)[i + j * m] = v;
       else ((float *)x)[i + j * m] = (float)v;
     }
 }
 
-static void call_once(void *a, void *b, void *c) {
-  const char *r = g_routine;
+static void call_once(const char *r, int dbl, void *a, void *b, void *c) {
   int m = g_m, n = g_n, k = g_k;
   double al = 0.75, be = 0.25;
   if (!strncmp(r, "gemm_", 5)) {
     int ta = r[5] == 't' ? TR : NT, tb = r[6] == 't' ? TR : NT;
     int lda = ta == NT ? m : k, ldb = tb == NT ? k : n;
-    if (g_dbl) ((gemm_d_t)sym("cblas_dgemm"))(COL, ta, tb, m, n, k, al, a, lda, b, ldb, be, c, m);
+    if (dbl) ((gemm_d_t)sym("cblas_dgemm"))(COL, ta, tb, m, n, k, al, a, lda, b, ldb, be, c, m);
     else ((gemm_s_t)sym("cblas_sgemm"))(COL, ta, tb, m, n, k, (float)al, a, lda, b, ldb, (float)be, c, m);
   } else if (!strcmp(r, "symm")) {
-    if (g_dbl) ((symm_d_t)sym("cblas_dsymm"))(COL, LEFT, LO, m, n, al, a, m, b, m, be, c, m);
+    if (dbl) ((symm_d_t)sym("cblas_dsymm"))(COL, LEFT, LO, m, n, al, a, m, b, m, be, c, m);
     else ((symm_s_t)sym("cblas_ssymm"))(COL, LEFT, LO, m, n, (float)al, a, m, b, m, (float)be, c, m);
   } else if (!strcmp(r, "syrk")) {
-    if (g_dbl) ((syrk_d_t)sym("cblas_dsyrk"))(COL, LO, NT, n, k, al, a, n, be, c, n);
+    if (dbl) ((syrk_d_t)sym("cblas_dsyrk"))(COL, LO, NT, n, k, al, a, n, be, c, n);
     else ((syrk_s_t)sym("cblas_ssyrk"))(COL, LO, NT, n, k, (float)al, a, n, (float)be, c, n);
   } else if (!strcmp(r, "syr2k")) {
-    if (g_dbl) ((symm_d_t)sym("cblas_dsyr2k"))(COL, LO, NT, n, k, al, a, n, b, n, be, c, n);
+    if (dbl) ((symm_d_t)sym("cblas_dsyr2k"))(COL, LO, NT, n, k, al, a, n, b, n, be, c, n);
     else ((symm_s_t)sym("cblas_ssyr2k"))(COL, LO, NT, n, k, (float)al, a, n, b, n, (float)be, c, n);
   } else if (!strcmp(r, "trmm") || !strcmp(r, "trsm")) {
-    const char *name = g_dbl ? (r[2] == 'm' ? "cblas_dtrmm" : "cblas_dtrsm")
+    const char *name = dbl ? (r[2] == 'm' ? "cblas_dtrmm" : "cblas_dtrsm")
                              : (r[2] == 'm' ? "cblas_strmm" : "cblas_strsm");
-    if (g_dbl) ((tr_d_t)sym(name))(COL, LEFT, LO, NT, NU, m, n, al, a, m, c, m);
+    if (dbl) ((tr_d_t)sym(name))(COL, LEFT, LO, NT, NU, m, n, al, a, m, c, m);
     else ((tr_s_t)sym(name))(COL, LEFT, LO, NT, NU, m, n, (float)al, a, m, c, m);
   } else {
     fprintf(stderr, "unknown routine %s\n", r);
@@ -102,34 +105,70 @@ static void call_once(void *a, void *b, void *c) {
   }
 }
 
-static void *worker(void *vp) {
-  long t = (long)vp;
-  size_t es = g_dbl ? 8 : 4;
+typedef struct {
+  const char *routine;
+  int dbl;
+  void *a, *b, *c, *c0;
+  size_t cbytes;
+} op_t;
+
+static void setup(op_t *op) {
+  size_t es = op->dbl ? 8 : 4;
   long m = g_m, n = g_n, k = g_k;
   long arows = m, acols = k, brows = k, bcols = n, crows = m, ccols = n;
-  const char *r = g_routine;
+  const char *r = op->routine;
   if (!strcmp(r, "symm") || !strncmp(r, "tr", 2)) { acols = m; brows = m; }
   if (!strncmp(r, "syr", 3)) { arows = n; acols = k; brows = n; bcols = k; crows = n; ccols = n; }
   if (!strncmp(r, "gemm_", 5)) {
     if (r[5] == 't') { arows = k; acols = m; }
     if (r[6] == 't') { brows = n; bcols = k; }
   }
-  void *a = malloc(es * arows * acols), *b = malloc(es * brows * bcols);
-  void *c = malloc(es * crows * ccols), *c0 = malloc(es * crows * ccols);
-  fill(a, arows, acols, 0, !strcmp(r, "trsm"));
-  fill(b, brows, bcols, 1, 0);
-  fill(c0, crows, ccols, 2, 0);
-  for (int w = 0; w < g_warmup; ++w) { memcpy(c, c0, es * crows * ccols); call_once(a, b, c); }
+  op->a = malloc(es * arows * acols);
+  op->b = malloc(es * brows * bcols);
+  op->c = malloc(es * crows * ccols);
+  op->c0 = malloc(es * crows * ccols);
+  op->cbytes = es * crows * ccols;
+  fill(op->dbl, op->a, arows, acols, 0, !strcmp(r, "trsm"));
+  fill(op->dbl, op->b, brows, bcols, 1, 0);
+  fill(op->dbl, op->c0, crows, ccols, 2, 0);
+}
+
+static void run_op(op_t *op) {
+  memcpy(op->c, op->c0, op->cbytes);
+  call_once(op->routine, op->dbl, op->a, op->b, op->c);
+}
+
+static void *worker(void *vp) {
+  long t = (long)vp;
+  int family = !strcmp(g_routine, "family");
+  int nops = family ? 18 : 1;
+  op_t ops[18];
+  for (int q = 0; q < nops; ++q) {
+    ops[q].routine = family ? FAMILY[q % 9] : g_routine;
+    ops[q].dbl = family ? q >= 9 : g_dbl;
+    setup(&ops[q]);
+  }
+  for (int w = 0; w < g_warmup; ++w)
+    for (int q = 0; q < nops; ++q) run_op(&ops[q]);
   pthread_barrier_wait(&g_start);
-  for (int q = 0; q < g_reps; ++q) {
-    memcpy(c, c0, es * crows * ccols);
+  for (int r = 0; r < g_reps; ++r) {
     double t0 = now();
-    call_once(a, b, c);
-    g_times[t * g_reps + q] = now() - t0;
+    for (int q = 0; q < nops; ++q) run_op(&ops[q]);
+    g_times[t * g_reps + r] = now() - t0;
   }
   pthread_barrier_wait(&g_done);
-  free(a); free(b); free(c); free(c0);
+  for (int q = 0; q < nops; ++q) {
+    free(ops[q].a); free(ops[q].b); free(ops[q].c); free(ops[q].c0);
+  }
   return NULL;
+}
+
+static double flops_of(const char *r, double m, double n, double k) {
+  if (!strncmp(r, "gemm", 4)) return 2 * m * n * k;
+  if (!strcmp(r, "symm")) return 2 * m * m * n;
+  if (!strcmp(r, "syrk")) return n * (n + 1) * k;
+  if (!strcmp(r, "syr2k")) return 2 * n * (n + 1) * k;
+  return m * m * n;
 }
 
 static int cmp(const void *x, const void *y) {
@@ -160,13 +199,12 @@ int main(int argc, char **argv) {
   double wall = now() - t0;
   for (int t = 0; t < g_threads; ++t) pthread_join(tid[t], NULL);
 
-  double m = g_m, n = g_n, k = g_k, flops;
+  double flops = 0;
   const char *r = g_routine;
-  if (!strncmp(r, "gemm", 4)) flops = 2 * m * n * k;
-  else if (!strcmp(r, "symm")) flops = 2 * m * m * n;
-  else if (!strcmp(r, "syrk")) flops = n * (n + 1) * k;
-  else if (!strcmp(r, "syr2k")) flops = 2 * n * (n + 1) * k;
-  else flops = m * m * n;
+  if (!strcmp(r, "family"))
+    for (int q = 0; q < 18; ++q) flops += flops_of(FAMILY[q % 9], g_m, g_n, g_k);
+  else
+    flops = flops_of(r, g_m, g_n, g_k);
   int total = g_threads * g_reps;
   qsort(g_times, (size_t)total, sizeof(double), cmp);
   double median = g_times[total / 2];

@@ -93,7 +93,8 @@ def ld(x, order):
     if x is None:
         return 1
     axis = 0 if order == "C" else 1
-    if x.size == 0:
+    if x.size == 0 or x.shape[axis] == 1:
+        # a single row/column: the stride along it is meaningless
         return max(1, x.shape[1 - axis])
     return max(1, x.strides[axis] // x.itemsize)
 
