@@ -55,6 +55,29 @@ int mublis_b200_fill_s(float *x, long m, long n, long ld, uint32_t seed, uint32_
 int mublis_b200_fill_d(double *x, long m, long n, long ld, uint32_t seed, uint32_t matrix_id,
                        int kind);
 
+/* SGEMM that allocates no memory.  No counterpart in the reference (its
+ * CPU library draws packing buffers from a host pool, frame/base/pool.c).
+ *
+ * For callers that cannot allocate device memory when they call in: a
+ * process whose GPU memory is already owned by another allocator, or a
+ * service that keeps a fixed device footprint and bans cudaMalloc/cudaFree
+ * on its request path.  Same arguments and result as mublis_sgemm, but A, B
+ * and C must be device pointers (staging host buffers would allocate), and
+ * the packed operand panels live in a fixed 32 MiB scratch array that is
+ * part of the library's device image, held on every GPU that loads the
+ * library until the process exits.  Limit:
+ *   (roundup(m, 128) + roundup(n, 128)) * roundup(k, 16) <= 8388608 floats
+ * (e.g. m = n = k = 2048); larger sizes return 1 with a message in
+ * mublis_b200_last_error() and leave C untouched.
+ * The first call on each device resolves the array's device address
+ * (cudaGetSymbolAddress with that device current); make that first call
+ * before any stream capture.  All calls on a device share the array and it
+ * keeps the last call's contents (nothing in it needs to start at zero);
+ * calls that overlap on the GPU race on it, so do not overlap them. */
+int mublis_b200_sgemm_noalloc(mublis_trans_t trans_a, mublis_trans_t trans_b, int m, int n, int k,
+                              float alpha, const float *a, int rs_a, int cs_a, const float *b,
+                              int rs_b, int cs_b, float beta, float *c, int rs_c, int cs_c);
+
 #ifdef __cplusplus
 }
 #endif

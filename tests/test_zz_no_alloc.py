@@ -1,0 +1,97 @@
+"""mublis_b200_sgemm_noalloc: the SGEMM entry point that allocates nothing.
+
+It exists for callers that cannot allocate device memory when they call in:
+processes whose GPU memory is already owned by another allocator, or services
+that keep a fixed device footprint and ban cudaMalloc/cudaFree on their
+request path.  Instead of per-call scratch it packs operands into a fixed
+32 MiB array that is part of the library's device image.
+
+Checked here, through the C ABI: two calls in a row (different shapes,
+transposes and inputs, so the second call runs over the first call's leftover
+scratch contents) agree with mublis_sgemm on the same device operands within
+the suite's tolerance (normwise relative error <= 4 * k * 2^-24); the second
+call leaves the device's free memory unchanged; sizes beyond the scratch
+limit are refused with a clear error and leave C untouched.
+
+This file is named to be collected last, so a failure here comes after every
+other test has run; it also passes on its own in a fresh process.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import mublis_b200 as mb
+
+pytestmark = pytest.mark.gpu
+
+_P, _I, _F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+NOALLOC_SIG = [_I, _I, _I, _I, _I, _F, _P, _I, _I, _P, _I, _I, _F, _P, _I, _I]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    lib = mb.load()
+    assert lib.mublis_b200_init() == 0, mb.last_error(lib)
+    lib.mublis_b200_sgemm_noalloc.argtypes = NOALLOC_SIG
+    lib.mublis_b200_sgemm_noalloc.restype = _I
+    lib.mublis_b200_set_form(b"s", b"plain")
+    return lib
+
+
+def _device_matrix(torch, lib, rows, cols, seed, matrix_id):
+    """rows x cols column-major FP32 device matrix (torch stores it transposed)."""
+    t = torch.empty(cols, rows, dtype=torch.float32, device="cuda")
+    assert lib.mublis_b200_fill_s(ctypes.c_void_p(t.data_ptr()), rows, cols, rows, seed,
+                                  matrix_id, 0) == 0
+    return t
+
+
+def _normwise(got, ref, a, b, c0, alpha, beta):
+    den = abs(alpha) * np.linalg.norm(a) * np.linalg.norm(b) + abs(beta) * np.linalg.norm(c0)
+    return np.linalg.norm(got.astype(np.float64) - ref.astype(np.float64)) / den
+
+
+def test_noalloc_matches_sgemm_on_two_calls_in_a_row(lib):
+    torch = pytest.importorskip("torch")
+    alpha, beta = 0.75, 0.25
+    calls = [(700, 513, 300, 0, 0, 11), (1024, 1000, 1024, 1, 1, 12)]
+    for i, (m, n, k, ta, tb, seed) in enumerate(calls):
+        a = _device_matrix(torch, lib, k if ta else m, m if ta else k, seed, 0)
+        b = _device_matrix(torch, lib, n if tb else k, k if tb else n, seed, 1)
+        c0 = _device_matrix(torch, lib, m, n, seed, 2)
+        c_ref, c_new = c0.clone(), c0.clone()
+        lda, ldb = (k if ta else m), (n if tb else k)
+        torch.cuda.synchronize()
+        st = lib.mublis_sgemm(ta, tb, m, n, k, alpha, a.data_ptr(), 1, lda, b.data_ptr(), 1, ldb,
+                              beta, c_ref.data_ptr(), 1, m)
+        assert st == 0, mb.last_error(lib)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        st = lib.mublis_b200_sgemm_noalloc(ta, tb, m, n, k, alpha, a.data_ptr(), 1, lda,
+                                           b.data_ptr(), 1, ldb, beta, c_new.data_ptr(), 1, m)
+        assert st == 0, mb.last_error(lib)
+        torch.cuda.synchronize()
+        if i == 1:  # the set-up happened on the first call; later calls allocate nothing
+            assert torch.cuda.mem_get_info()[0] == free_before
+        ref = c_ref.cpu().numpy().T
+        got = c_new.cpu().numpy().T
+        err = _normwise(got, ref, a.cpu().numpy(), b.cpu().numpy(), c0.cpu().numpy(), alpha, beta)
+        assert np.isfinite(got).all()
+        assert err <= 4 * k * 2.0 ** -24, (i, err)
+
+
+def test_noalloc_refuses_sizes_beyond_the_scratch_limit(lib):
+    torch = pytest.importorskip("torch")
+    m = n = k = 4096  # (4096 + 4096) * 4096 floats > 8 Mi floats
+    a = _device_matrix(torch, lib, m, k, 3, 0)
+    b = _device_matrix(torch, lib, k, n, 3, 1)
+    c = _device_matrix(torch, lib, m, n, 3, 2)
+    keep = c.clone()
+    torch.cuda.synchronize()
+    st = lib.mublis_b200_sgemm_noalloc(0, 0, m, n, k, 1.0, a.data_ptr(), 1, m, b.data_ptr(), 1, k,
+                                       0.5, c.data_ptr(), 1, m)
+    assert st != 0
+    assert "maximum" in mb.last_error(lib)
+    torch.cuda.synchronize()
+    assert torch.equal(c, keep)
