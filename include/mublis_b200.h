@@ -55,6 +55,51 @@ int mublis_b200_fill_s(float *x, long m, long n, long ld, uint32_t seed, uint32_
 int mublis_b200_fill_d(double *x, long m, long n, long ld, uint32_t seed, uint32_t matrix_id,
                        int kind);
 
+/* ---- grouped launches (no counterpart in the reference, which runs one
+ * call per host thread) -------------------------------------------------
+ * Many independent problems of one precision ('s' or 'd') in one persistent
+ * launch that walks a device-side problem table.  Operands must be device
+ * pointers; column-major with leading dimensions; alpha/beta are taken at
+ * the problem's precision.  Synchronous. */
+typedef struct {
+  int trans_a, trans_b; /* mublis_trans_t */
+  int m, n, k;
+  double alpha, beta;
+  const void *a;
+  int lda;
+  const void *b;
+  int ldb;
+  void *c;
+  int ldc;
+} mublis_b200_gemm_problem_t;
+
+/* Left-side solve op(A) X = alpha B, B overwritten (m x n, ldb). */
+typedef struct {
+  int uplo, trans_a, diag; /* mublis_uplo_t (LOWER/UPPER), mublis_trans_t, mublis_diag_t */
+  int m, n;
+  double alpha;
+  const void *a;
+  int lda;
+  void *b;
+  int ldb;
+} mublis_b200_trsm_problem_t;
+
+int mublis_b200_gemm_grouped(char dtype, const mublis_b200_gemm_problem_t *problems, int count);
+int mublis_b200_trsm_grouped(char dtype, const mublis_b200_trsm_problem_t *problems, int count);
+
+/* Plans: a grouped call over a fixed problem table (the same pointers and
+ * sizes every run).  Creation autotunes the tile shape per size class by
+ * timing every variant on the actual problems (C is restored afterwards)
+ * and captures the launches in a CUDA graph; run replays the graph on the
+ * calling thread's stream and waits for it. */
+typedef struct mublis_b200_plan mublis_b200_plan_t;
+int mublis_b200_plan_gemm_grouped(char dtype, const mublis_b200_gemm_problem_t *problems,
+                                  int count, mublis_b200_plan_t **plan);
+int mublis_b200_plan_trsm_grouped(char dtype, const mublis_b200_trsm_problem_t *problems,
+                                  int count, mublis_b200_plan_t **plan);
+int mublis_b200_plan_run(mublis_b200_plan_t *plan);
+int mublis_b200_plan_destroy(mublis_b200_plan_t *plan);
+
 /* SGEMM that allocates no memory.  No counterpart in the reference (its
  * CPU library draws packing buffers from a host pool, frame/base/pool.c).
  *

@@ -3,9 +3,9 @@
 // plus its micro-kernel (include/mublis_instantiate.h:37-52).
 //
 // One CTA per output tile (BM x BN), 256 threads, each thread an 8 x TN
-// register tile laid out CUTLASS-SIMT style (4 x 8 threads per warp, 4-wide
-// fragments) so every shared-memory fragment load is a broadcast or a single
-// 128-byte wavefront.  Operands come from packed MN-major panels (pack.cu)
+// register tile laid out CUTLASS-SIMT style (4 x 8 threads per warp,
+// 16-byte fragments spaced so that every shared-memory fragment load is a
+// broadcast or a single 128-byte wavefront).  Operands come from packed MN-major panels (pack.cu)
 // through a STAGES-deep cp.async pipeline; packing zero-pads every edge, so
 // the main loop has no bounds checks.
 //
@@ -32,14 +32,14 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ void lds4(float (&d)[4], const float *p) {
+// One 16-byte shared-memory fragment: 4 floats or 2 doubles.
+__device__ __forceinline__ void lds16(float (&d)[4], const float *p) {
   float4 v = *reinterpret_cast<const float4 *>(p);
   d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
 }
-__device__ __forceinline__ void lds4(double (&d)[4], const double *p) {
-  double2 v0 = *reinterpret_cast<const double2 *>(p);
-  double2 v1 = *reinterpret_cast<const double2 *>(p + 2);
-  d[0] = v0.x; d[1] = v0.y; d[2] = v1.x; d[3] = v1.y;
+__device__ __forceinline__ void lds16(double (&d)[2], const double *p) {
+  double2 v = *reinterpret_cast<const double2 *>(p);
+  d[0] = v.x; d[1] = v.y;
 }
 
 template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB>
@@ -47,11 +47,15 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
   constexpr int NT = 256;
   constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;
   constexpr int TM = WTM / 4, TN = WTN / 8;
-  constexpr int MCH = TM / 4, NCH = TN / 4;
-  constexpr int MSP = WTM / MCH, NSP = WTN / NCH;  // chunk spacing
-  constexpr int VEC = 16 / sizeof(T);
+  // Fragments are 16-byte chunks of CW elements; a thread's chunks are
+  // spaced so that one warp-wide load touches 4 (A) or 8 (B) consecutive
+  // chunks: a single 128-byte wavefront, no bank conflicts.
+  constexpr int CW = 16 / sizeof(T);
+  constexpr int MCH = TM / CW, NCH = TN / CW;
+  constexpr int MSP = 4 * CW, NSP = 8 * CW;  // chunk spacing
+  constexpr int VEC = CW;
   static_assert(WARPS_M * WARPS_N == 8, "8 warps");
-  static_assert(TM % 4 == 0 && TN % 4 == 0, "4-wide fragments");
+  static_assert(TM % CW == 0 && TN % CW == 0, "16-byte fragments");
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *As = reinterpret_cast<T *>(smem_raw);
@@ -121,24 +125,24 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
     cp_async_commit();
 
     const int st = (kt - kt_begin) % STAGES;
-    const T *sa = As + st * BK * BM + wm * WTM + ty * 4;
-    const T *sb = Bs + st * BK * BN + wn * WTN + tx * 4;
+    const T *sa = As + st * BK * BM + wm * WTM + ty * CW;
+    const T *sb = Bs + st * BK * BN + wn * WTN + tx * CW;
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       T af[TM], bf[TN];
 #pragma unroll
       for (int mc = 0; mc < MCH; ++mc) {
-        T t[4];
-        lds4(t, sa + kk * BM + mc * MSP);
+        T t[CW];
+        lds16(t, sa + kk * BM + mc * MSP);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) af[mc * 4 + q] = t[q];
+        for (int q = 0; q < CW; ++q) af[mc * CW + q] = t[q];
       }
 #pragma unroll
       for (int nc = 0; nc < NCH; ++nc) {
-        T t[4];
-        lds4(t, sb + kk * BN + nc * NSP);
+        T t[CW];
+        lds16(t, sb + kk * BN + nc * NSP);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) bf[nc * 4 + q] = t[q];
+        for (int q = 0; q < CW; ++q) bf[nc * CW + q] = t[q];
       }
 #pragma unroll
       for (int i = 0; i < TM; ++i)
@@ -151,11 +155,11 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
   const T alpha = p.alpha, beta = p.beta;
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
-    const long gi = m0 + wm * WTM + (i / 4) * MSP + ty * 4 + (i % 4);
+    const long gi = m0 + wm * WTM + (i / CW) * MSP + ty * CW + (i % CW);
     if (gi >= p.m) continue;
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      const long gj = n0 + wn * WTN + (j / 4) * NSP + tx * 4 + (j % 4);
+      const long gj = n0 + wn * WTN + (j / CW) * NSP + tx * CW + (j % CW);
       if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
       T *cij = p.c + gi * p.rs_c + gj * p.cs_c;
       T v = alpha * acc[i][j];

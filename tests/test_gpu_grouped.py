@@ -1,0 +1,195 @@
+"""Grouped launches (config 4 style): many independent GEMMs / TRSMs of
+uneven sizes in one persistent launch, and plans (autotuned tiles + CUDA
+graph replay).
+
+Each grouped result is compared with the library's single-call path on the
+same device operands (normwise relative error <= 4 * k * u, the suite's
+tolerance) and, for a few problems, with the oracle restatement.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import mublis_b200 as mb
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+class GemmProblem(ctypes.Structure):
+    _fields_ = [("trans_a", ctypes.c_int), ("trans_b", ctypes.c_int), ("m", ctypes.c_int),
+                ("n", ctypes.c_int), ("k", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double), ("a", ctypes.c_void_p), ("lda", ctypes.c_int),
+                ("b", ctypes.c_void_p), ("ldb", ctypes.c_int), ("c", ctypes.c_void_p),
+                ("ldc", ctypes.c_int)]
+
+
+class TrsmProblem(ctypes.Structure):
+    _fields_ = [("uplo", ctypes.c_int), ("trans_a", ctypes.c_int), ("diag", ctypes.c_int),
+                ("m", ctypes.c_int), ("n", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("a", ctypes.c_void_p), ("lda", ctypes.c_int), ("b", ctypes.c_void_p),
+                ("ldb", ctypes.c_int)]
+
+
+@pytest.fixture(scope="module")
+def glib():
+    lib = mb.load()
+    assert lib.mublis_b200_init() == 0, mb.last_error(lib)
+    P = ctypes.POINTER
+    lib.mublis_b200_gemm_grouped.argtypes = [ctypes.c_char, P(GemmProblem), ctypes.c_int]
+    lib.mublis_b200_trsm_grouped.argtypes = [ctypes.c_char, P(TrsmProblem), ctypes.c_int]
+    lib.mublis_b200_plan_gemm_grouped.argtypes = [ctypes.c_char, P(GemmProblem), ctypes.c_int,
+                                                  P(ctypes.c_void_p)]
+    lib.mublis_b200_plan_trsm_grouped.argtypes = [ctypes.c_char, P(TrsmProblem), ctypes.c_int,
+                                                  P(ctypes.c_void_p)]
+    lib.mublis_b200_plan_run.argtypes = [ctypes.c_void_p]
+    lib.mublis_b200_plan_destroy.argtypes = [ctypes.c_void_p]
+    for p in (b"s", b"d"):
+        lib.mublis_b200_set_form(p, b"plain")
+    return lib
+
+
+def log_uniform_int(rng, lo, hi, size):
+    return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size))).astype(int)
+
+
+def make_gemm_set(torch, p, count, seed, lo=16, hi=512):
+    dt = torch.float32 if p == "s" else torch.float64
+    rng = np.random.default_rng(seed)
+    mnk = log_uniform_int(rng, lo, hi, (count, 3))
+    probs, keep = [], []
+    for q in range(count):
+        m, n, k = (int(x) for x in mnk[q])
+        ta, tb = int(rng.integers(0, 2)), int(rng.integers(0, 2))
+        a = torch.rand((m, k) if ta else (k, m), dtype=dt, device="cuda") * 2 - 1
+        b = torch.rand((k, n) if tb else (n, k), dtype=dt, device="cuda") * 2 - 1
+        c = torch.rand((n, m), dtype=dt, device="cuda") * 2 - 1
+        al, be = rng.uniform(0.5, 1.5, 2)
+        # torch tensors are row-major: a (rows, cols) row-major buffer is the
+        # column-major transpose, so lda is the row length.
+        probs.append(GemmProblem(ta, tb, m, n, k, al, be, a.data_ptr(), a.shape[1], b.data_ptr(),
+                                 b.shape[1], c.data_ptr(), m))
+        keep.append((a, b, c))
+    return probs, keep
+
+
+def single_call(lib, p, pr):
+    fn = getattr(lib, f"mublis_{p}gemm")
+    return fn(pr.trans_a, pr.trans_b, pr.m, pr.n, pr.k, pr.alpha, pr.a, 1, pr.lda, pr.b, 1,
+              pr.ldb, pr.beta, pr.c, 1, pr.ldc)
+
+
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_grouped_gemm_matches_single_calls(glib, p):
+    torch = pytest.importorskip("torch")
+    probs, keep = make_gemm_set(torch, p, 96, seed=1)
+    c0 = [c.clone() for _, _, c in keep]
+    arr = (GemmProblem * len(probs))(*probs)
+    assert glib.mublis_b200_gemm_grouped(p.encode(), arr, len(probs)) == 0, mb.last_error(glib)
+    grouped = [c.clone() for _, _, c in keep]
+    u = 2.0 ** -24 if p == "s" else 2.0 ** -53
+    for q, pr in enumerate(probs):
+        keep[q][2].copy_(c0[q])
+        assert single_call(glib, p, pr) == 0
+        a, b, _ = keep[q]
+        den = abs(pr.alpha) * a.norm().item() * b.norm().item() + abs(pr.beta) * c0[q].norm().item()
+        err = (grouped[q].double() - keep[q][2].double()).norm().item() / den
+        assert err <= 4 * pr.k * u, (q, pr.m, pr.n, pr.k, err)
+
+
+def test_grouped_gemm_against_oracle(glib):
+    torch = pytest.importorskip("torch")
+    m, n, k = 37, 129, 200
+    a = orc.fill(m, k, np.float32, 5, 0)
+    b = orc.fill(k, n, np.float32, 5, 1)
+    c0 = orc.fill(m, n, np.float32, 5, 2)
+    ta, tb, tc = (torch.from_numpy(x.T.copy()).cuda() for x in (a, b, c0))
+    pr = GemmProblem(0, 0, m, n, k, 0.75, 0.25, ta.data_ptr(), m, tb.data_ptr(), k,
+                     tc.data_ptr(), m)
+    assert glib.mublis_b200_gemm_grouped(b"s", (GemmProblem * 1)(pr), 1) == 0
+    ref = c0.copy(order="F")
+    assert orc.restated().oracle_sgemm(0, 0, m, n, k, 0.75, a.ctypes.data, 1, m, b.ctypes.data,
+                                       1, k, 0.25, ref.ctypes.data, 1, m) == 0
+    got = tc.cpu().numpy().T
+    err = np.linalg.norm(got - ref) / (0.75 * np.linalg.norm(a) * np.linalg.norm(b) +
+                                       0.25 * np.linalg.norm(c0))
+    assert err <= 4 * k * 2.0 ** -24
+
+
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_plan_replay_equals_grouped_call(glib, p):
+    torch = pytest.importorskip("torch")
+    probs, keep = make_gemm_set(torch, p, 64, seed=3)
+    c0 = [c.clone() for _, _, c in keep]
+    arr = (GemmProblem * len(probs))(*probs)
+    plan = ctypes.c_void_p()
+    assert glib.mublis_b200_plan_gemm_grouped(p.encode(), arr, len(probs), ctypes.byref(plan)) == 0
+    # planning (autotuning trials included) leaves C as it was
+    for q in range(len(probs)):
+        assert torch.equal(keep[q][2], c0[q])
+    assert glib.mublis_b200_plan_run(plan) == 0
+    replay = [c.clone() for _, _, c in keep]
+    for q in range(len(probs)):
+        keep[q][2].copy_(c0[q])
+    assert glib.mublis_b200_gemm_grouped(p.encode(), arr, len(probs)) == 0
+    for q in range(len(probs)):
+        assert torch.equal(replay[q], keep[q][2])  # same tiles -> bit-identical
+    assert glib.mublis_b200_plan_destroy(plan) == 0
+
+
+def make_trsm_set(torch, p, count, seed):
+    dt = torch.float32 if p == "s" else torch.float64
+    rng = np.random.default_rng(seed)
+    orders = log_uniform_int(rng, 32, 256, count)
+    nrhs = log_uniform_int(rng, 1, 128, count)
+    probs, keep = [], []
+    for q in range(count):
+        m, n = int(orders[q]), int(nrhs[q])
+        a = (torch.rand(m, m, dtype=dt, device="cuda") * 2 - 1) / m
+        a.diagonal().copy_(torch.rand(m, dtype=dt, device="cuda") + 1)
+        b = torch.rand(n, m, dtype=dt, device="cuda") * 2 - 1
+        uplo = mb.M_LOWER if q % 2 == 0 else mb.M_UPPER
+        trans = q % 3 == 0
+        diag = mb.M_UNIT if q % 5 == 0 else mb.M_NON_UNIT
+        probs.append(TrsmProblem(uplo, int(trans), diag, m, n, float(rng.uniform(0.5, 1.5)),
+                                 a.data_ptr(), m, b.data_ptr(), m))
+        keep.append((a, b))
+    return probs, keep
+
+
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_grouped_trsm_matches_single_calls(glib, p):
+    torch = pytest.importorskip("torch")
+    probs, keep = make_trsm_set(torch, p, 48, seed=4)
+    b0 = [b.clone() for _, b in keep]
+    arr = (TrsmProblem * len(probs))(*probs)
+    assert glib.mublis_b200_trsm_grouped(p.encode(), arr, len(probs)) == 0, mb.last_error(glib)
+    grouped = [b.clone() for _, b in keep]
+    u = 2.0 ** -24 if p == "s" else 2.0 ** -53
+    fn = getattr(glib, f"mublis_{p}trsm")
+    for q, pr in enumerate(probs):
+        keep[q][1].copy_(b0[q])
+        assert fn(mb.M_LEFT, pr.uplo, pr.trans_a, pr.diag, pr.m, pr.n, pr.alpha, pr.a, 1, pr.lda,
+                  pr.b, 1, pr.ldb) == 0
+        ref = keep[q][1].double()
+        err = (grouped[q].double() - ref).norm().item() / ref.norm().item()
+        assert err <= 4 * pr.m * u, (q, pr.m, pr.n, err)
+
+
+@pytest.mark.parametrize("p", ["s", "d"])
+def test_trsm_plan_replay(glib, p):
+    torch = pytest.importorskip("torch")
+    probs, keep = make_trsm_set(torch, p, 32, seed=6)
+    b0 = [b.clone() for _, b in keep]
+    arr = (TrsmProblem * len(probs))(*probs)
+    plan = ctypes.c_void_p()
+    assert glib.mublis_b200_plan_trsm_grouped(p.encode(), arr, len(probs), ctypes.byref(plan)) == 0
+    assert glib.mublis_b200_plan_run(plan) == 0
+    replay = [b.clone() for _, b in keep]
+    for q in range(len(probs)):
+        keep[q][1].copy_(b0[q])
+    assert glib.mublis_b200_trsm_grouped(p.encode(), arr, len(probs)) == 0
+    for q in range(len(probs)):
+        assert torch.equal(replay[q], keep[q][1])
+    assert glib.mublis_b200_plan_destroy(plan) == 0
