@@ -51,7 +51,7 @@ COL, NT, TR, UPPER, LOWER, NONUNIT, LEFT = 102, 111, 112, 121, 122, 131, 141
 ALPHA, BETA = 0.75, 0.25
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # SMs x FP64 FMA lanes x 2 x max clock
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs x FP32 FMA lanes x 2 x max clock
-LEAF = 32  # TRSM diagonal-block leaf size (rows) of the device solve
+LEAF = 64  # TRSM diagonal-block leaf size (rows) of the device solve
 
 
 def flops(routine: str, n: int) -> float:
@@ -70,11 +70,20 @@ def family_flops(n: int) -> float:
     return 2 * sum(flops(r, n) for r in ROUTINES)
 
 
+DIRECT_K = 256  # TRSM updates with k <= this read operands directly (no pack)
+
+
 def kernel_flops(n: int) -> dict:
-    """Flops of one step attributed to the kernel that executes them."""
-    gemm_part = sum(flops(r, n) for r in ROUTINES if r != "trsm") + (n ** 3 - LEAF * n * n)
+    """Algorithmic flops of one step attributed to the kernel that executes
+    them.  The recursive TRSM of order n (a power of two) halves down to
+    LEAF-row diagonal blocks: updates of half-order h > DIRECT_K (sum of h =
+    n - 2*DIRECT_K) run on the packed GEMM kernel, the thinner updates (sum
+    2*DIRECT_K - LEAF) and the leaf solves (LEAF * n^2, done as products with
+    the inverted diagonal blocks) on the direct kernel."""
+    gemm_part = sum(flops(r, n) for r in ROUTINES if r != "trsm") + n * n * (n - 2 * DIRECT_K)
+    direct = float(n * n * 2 * DIRECT_K)
     return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part,
-            "trsm_leaf_s": float(LEAF * n * n), "trsm_leaf_d": float(LEAF * n * n)}
+            "direct_sgemm": direct, "direct_dgemm": direct}
 
 
 def measured_peaks() -> dict:
@@ -302,6 +311,208 @@ def forms_study(torch, lib) -> dict:
     return out
 
 
+def _log_uniform_int(rng, lo, hi, size):
+    import numpy as np
+    return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size))).astype(int)
+
+
+def grouped_study(torch, lib) -> dict:
+    """Config 4: 4096 independent SGEMMs with m, n, k log-uniform over [16, 512]
+    (seed 1), column-major, lda = m, per-problem alpha, beta uniform[0.5, 1.5);
+    and 1024 DTRSMs (left, lower, non-unit) with order log-uniform in [32, 256],
+    right-hand sides log-uniform in [1, 128], A off-diagonal uniform/n and
+    diagonal in [1, 2).  One persistent grouped launch per plan (tiles
+    autotuned, CUDA-graph replay) against one library call per problem."""
+    import numpy as np
+    import mublis_b200 as mb
+    rng = np.random.default_rng(1)
+    torch.manual_seed(1)
+    mnk = _log_uniform_int(rng, 16, 512, (4096, 3))
+    ab = rng.uniform(0.5, 1.5, (4096, 2))
+    probs, keep = [], []
+    for q in range(4096):
+        m, n, k = (int(x) for x in mnk[q])
+        a = torch.rand(k, m, device="cuda") * 2 - 1
+        b = torch.rand(n, k, device="cuda") * 2 - 1
+        c = torch.rand(n, m, device="cuda") * 2 - 1
+        probs.append(mb.GemmProblem(0, 0, m, n, k, ab[q, 0], ab[q, 1], a.data_ptr(), m,
+                                    b.data_ptr(), k, c.data_ptr(), m))
+        keep.append((a, b, c))
+    gflop = sum(2.0 * p.m * p.n * p.k for p in probs)
+    arr = (mb.GemmProblem * len(probs))(*probs)
+    plan = ctypes.c_void_p()
+    mb.check(lib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)), lib)
+    ms_plan = timed(torch, lambda: lib.mublis_b200_plan_run(plan), 10)
+
+    def loop():
+        for p in probs:
+            lib.mublis_sgemm(0, 0, p.m, p.n, p.k, p.alpha, p.a, 1, p.lda, p.b, 1, p.ldb, p.beta,
+                             p.c, 1, p.ldc)
+    ms_loop = timed(torch, loop, 2)
+    lib.mublis_b200_plan_destroy(plan)
+    del keep
+    orders = _log_uniform_int(rng, 32, 256, 1024)
+    nrhs = _log_uniform_int(rng, 1, 128, 1024)
+    tp, tk = [], []
+    for q in range(1024):
+        m, n = int(orders[q]), int(nrhs[q])
+        a = (torch.rand(m, m, dtype=torch.float64, device="cuda") * 2 - 1) / m
+        a.diagonal().copy_(torch.rand(m, dtype=torch.float64, device="cuda") + 1)
+        b = torch.rand(n, m, dtype=torch.float64, device="cuda") * 2 - 1
+        tp.append(mb.TrsmProblem(mb.M_LOWER, 0, mb.M_NON_UNIT, m, n, 1.0, a.data_ptr(), m,
+                                 b.data_ptr(), m))
+        tk.append((a, b))
+    tflop = sum(float(p.m) ** 2 * p.n for p in tp)
+    tarr = (mb.TrsmProblem * len(tp))(*tp)
+    tplan = ctypes.c_void_p()
+    mb.check(lib.mublis_b200_plan_trsm_grouped(b"d", tarr, len(tp), ctypes.byref(tplan)), lib)
+    ms_tplan = timed(torch, lambda: lib.mublis_b200_plan_run(tplan), 10)
+
+    def tloop():
+        for p in tp:
+            lib.mublis_dtrsm(0, p.uplo, 0, 0, p.m, p.n, 1.0, p.a, 1, p.lda, p.b, 1, p.ldb)
+    ms_tloop = timed(torch, tloop, 2)
+    lib.mublis_b200_plan_destroy(tplan)
+    del tk
+    torch.cuda.empty_cache()
+    return {"sgemm_x4096": {"gflop": round(gflop / 1e9, 2), "grouped_ms": round(ms_plan, 3),
+                            "grouped_tflops": round(gflop / ms_plan / 1e9, 2),
+                            "one_call_per_launch_ms": round(ms_loop, 2),
+                            "speedup": round(ms_loop / ms_plan, 1)},
+            "dtrsm_x1024": {"gflop": round(tflop / 1e9, 3), "grouped_ms": round(ms_tplan, 3),
+                            "one_call_per_launch_ms": round(ms_tloop, 2),
+                            "speedup": round(ms_tloop / ms_tplan, 1)}}
+
+
+def served_study(torch, lib, nreq: int = 400) -> dict:
+    """Config 5: 16 host threads issue cblas calls with Poisson arrivals
+    (aggregate 20k calls/s, seed 2); mix 60% SGEMM, 20% DGEMM, 10% SSYRK, 10%
+    DTRSM; 80% of sizes log-uniform in [32, 256], 20% from {1024, 2048, 4096,
+    8192}; operands device-resident in server handles under a 64 GiB HBM
+    budget.  Served (request server attached, "auto" forms) against the same
+    requests issued as serialized plain calls at the same arrival times.
+    Latency = completion - scheduled arrival."""
+    import threading
+    import numpy as np
+    import mublis_b200 as mb
+    rng = np.random.default_rng(2)
+    arrivals = np.cumsum(rng.exponential(1 / 20000.0, nreq))
+    kinds = rng.choice(["sgemm", "dgemm", "ssyrk", "dtrsm"], p=[0.6, 0.2, 0.1, 0.1], size=nreq)
+    cfg = mb.ServerConfig(hbm_budget_bytes=64 << 30, streams=4, batch_window_us=100,
+                          small_max_dim=512, max_batch=4096, sform=b"auto", dform=b"auto")
+    srv = ctypes.c_void_p()
+    mb.check(lib.mublis_b200_server_create(ctypes.byref(cfg), ctypes.byref(srv)), lib)
+    reqs, extra = [], []
+    try:
+        for q in range(nreq):
+            if rng.random() < 0.8:
+                m, n, k = (int(x) for x in np.floor(np.exp(rng.uniform(np.log(32), np.log(257), 3))))
+            else:
+                m = n = k = int(rng.choice([1024, 2048, 4096, 8192]))
+            kind = kinds[q]
+            p = kind[0]
+            elt = 4 if p == "s" else 8
+            fill = getattr(lib, f"mublis_b200_fill_{p}")
+            if kind.endswith("gemm"):
+                shapes, fl = [(m, k), (k, n), (m, n)], 2.0 * m * n * k
+            elif kind == "ssyrk":
+                m = n
+                shapes, fl = [(n, k), (n, n)], float(n) * (n + 1) * k
+            else:
+                shapes, fl = [(m, m), (m, n)], float(m) * m * n
+            ptrs = []
+            for i, (r, c) in enumerate(shapes):
+                d = ctypes.c_void_p()
+                mb.check(lib.mublis_b200_server_alloc(srv, r * c * elt, ctypes.byref(d)), lib)
+                mb.check(fill(d, r, c, r, q, i, 0), lib)
+                ptrs.append(d.value)
+            if kind == "dtrsm":  # well-conditioned triangle in the handle
+                a = torch.empty(m, m, dtype=torch.float64, device="cuda")
+                dg = torch.empty(m, m, dtype=torch.float64, device="cuda")
+                lib.mublis_b200_fill_d(ctypes.c_void_p(a.data_ptr()), m, m, m, q, 0, 0)
+                lib.mublis_b200_fill_d(ctypes.c_void_p(dg.data_ptr()), m, m, m, q, 9, 2)
+                a.div_(m)
+                a.diagonal().copy_(dg.diagonal())
+                extra.append(a)
+                ptrs[0] = a.data_ptr()
+                del dg
+            reqs.append(dict(kind=kind, m=m, n=n, k=k, p=ptrs, fl=fl, at=float(arrivals[q])))
+        torch.cuda.synchronize()
+        P = ctypes.c_void_p
+
+        def issue(r):
+            k_, m, n, p = r["kind"], r["m"], r["n"], r["p"]
+            if k_ == "sgemm":
+                lib.cblas_sgemm(COL, NT, NT, m, n, r["k"], 0.75, P(p[0]), m, P(p[1]), r["k"], 0.25,
+                                P(p[2]), m)
+            elif k_ == "dgemm":
+                lib.cblas_dgemm(COL, NT, NT, m, n, r["k"], 0.75, P(p[0]), m, P(p[1]), r["k"], 0.25,
+                                P(p[2]), m)
+            elif k_ == "ssyrk":
+                lib.cblas_ssyrk(COL, LOWER, NT, n, r["k"], 0.75, P(p[0]), n, 0.25, P(p[1]), n)
+            else:
+                lib.cblas_dtrsm(COL, LEFT, LOWER, NT, NONUNIT, m, n, 0.75, P(p[0]), m, P(p[1]), m)
+
+        def serial():
+            for pp in (b"s", b"d"):
+                lib.mublis_b200_set_form(pp, b"plain")
+            lat = [0.0] * nreq
+            t0 = time.perf_counter()
+            for q, r in enumerate(reqs):
+                target = t0 + r["at"]
+                while time.perf_counter() < target:
+                    pass
+                issue(r)
+                lat[q] = time.perf_counter() - target
+            return lat, time.perf_counter() - t0
+
+        def served():
+            lib.mublis_b200_server_attach(srv)
+            lib.mublis_b200_server_reset_stats(srv)
+            lat = [0.0] * nreq
+            t0 = time.perf_counter() + 0.05
+
+            def worker(t):
+                for q in range(t, nreq, 16):
+                    target = t0 + reqs[q]["at"]
+                    while time.perf_counter() < target:
+                        pass
+                    issue(reqs[q])
+                    lat[q] = time.perf_counter() - target
+            ths = [threading.Thread(target=worker, args=(t,)) for t in range(16)]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            span = time.perf_counter() - t0
+            lib.mublis_b200_server_attach(None)
+            st = mb.ServerStats()
+            lib.mublis_b200_server_stats(srv, ctypes.byref(st))
+            return lat, span, st
+
+        serial()
+        served()  # warm-up of both paths (module loads, tuned tiles, pools)
+        lat_s, span_s = serial()
+        lat_v, span_v, st = served()
+        tot = sum(r["fl"] for r in reqs)
+        pct = lambda l, q: round(float(np.percentile(l, q)) * 1e3, 2)  # noqa: E731
+        return {"requests": nreq, "tflop": round(tot / 1e12, 2),
+                "served": {"tflops": round(tot / span_v / 1e12, 2), "p50_ms": pct(lat_v, 50),
+                           "p99_ms": pct(lat_v, 99), "batches": int(st.batches),
+                           "batched_requests": int(st.batched_requests),
+                           "forms": "auto (bf16x6 / ozaki:8 above crossover, else plain)"},
+                "serialized_plain": {"tflops": round(tot / span_s / 1e12, 2),
+                                     "p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99)},
+                "throughput_ratio": round(span_s / span_v, 2)}
+    finally:
+        lib.mublis_b200_server_attach(None)
+        lib.mublis_b200_server_destroy(srv)
+        for pp in (b"s", b"d"):
+            lib.mublis_b200_set_form(pp, b"plain")
+        del extra
+        torch.cuda.empty_cache()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -311,6 +522,8 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--no-forms", action="store_true", help="skip the 8192 precision-form study")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="skip the grouped (config 4) and served (config 5) studies")
     ap.add_argument("--only-timed", action="store_true",
                     help="warm-up + timed steps only (for profiler launch lists)")
     args = ap.parse_args()
@@ -372,7 +585,7 @@ def main():
 
     # per-routine breakdown (untimed by the headline; one pass, event per call)
     if args.only_timed:
-        args.no_forms = args.no_cpu = True
+        args.no_forms = args.no_cpu = args.no_studies = True
     breakdown = {}
     if rank == 0 and not args.only_timed:
         for (p, r, ops), _ in zip(fam.calls, range(len(fam.calls))):
@@ -422,6 +635,10 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = forms_study(torch, lib)
+    grouped = served = None
+    if rank == 0 and world == 1 and not args.no_studies:
+        grouped = grouped_study(torch, lib)
+        served = served_study(torch, lib)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -447,7 +664,7 @@ def main():
                 "stated_err": "normwise relative error <= 4*k*u against the oracle "
                               "(tests/test_gpu_parity.py); measured plain SGEMM ~1.9e-8, "
                               "DGEMM ~3.4e-17 at 8192 (profiles/precision_forms_8192.md)",
-                "forms_8192_tflops": forms,
+                "forms_8192_tflops": forms, "grouped_config4": grouped, "served_config5": served,
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in kstats.items()}}
         print(json.dumps(line))
     if world > 1:

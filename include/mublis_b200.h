@@ -37,6 +37,9 @@ void *mublis_b200_get_stream(void);
  *        products, FP32 accumulate), "bf16x6" (3-term split, 6 products)
  *   'd': "plain" (FP64 FMA pipe), "ozaki" or "ozaki:<slices>" (int8 slices,
  *        exact int32 tensor-core accumulation, FP64 recombination)
+ *   both: "auto" -- per call, the fastest form whose error is no worse than
+ *        plain: FP32 uses bf16x6 when min(m, n) and k are >= 512, FP64 uses
+ *        ozaki:8 when min(m, n) and k are >= 4096, plain otherwise
  * Also settable with MUBLIS_B200_SFORM / MUBLIS_B200_DFORM. */
 int mublis_b200_set_form(char dtype, const char *form);
 
@@ -99,6 +102,46 @@ int mublis_b200_plan_trsm_grouped(char dtype, const mublis_b200_trsm_problem_t *
                                   int count, mublis_b200_plan_t **plan);
 int mublis_b200_plan_run(mublis_b200_plan_t *plan);
 int mublis_b200_plan_destroy(mublis_b200_plan_t *plan);
+
+/* ---- request server (no counterpart in the reference) -------------------
+ * Continuous batching of Level-3 calls issued by many host threads.  Once a
+ * server is attached, every cblas_* / mublis_* call whose operands are ALL
+ * device-resident becomes a request: the calling thread blocks until it
+ * completes (calls stay synchronous), while the server's scheduler thread
+ * coalesces small plain GEMMs (max(m,n,k) <= small_max_dim) and small left
+ * TRSMs (order <= 256) waiting together into one grouped launch per
+ * precision, and issues the rest asynchronously on a pool of streams,
+ * admitting each when its scratch estimate fits the HBM budget.  Calls with
+ * host operands keep the direct path. */
+typedef struct {
+  size_t hbm_budget_bytes; /* device memory for handles + scratch (0: 64 GiB) */
+  int streams;             /* concurrent streams (0: 4) */
+  int batch_window_us;     /* extra wait for small arrivals to coalesce (0: none) */
+  int small_max_dim;       /* batchable GEMM size limit (0: 512) */
+  int max_batch;           /* requests per grouped launch (0: 4096) */
+  const char *sform;       /* precision form for non-batched FP32 work (NULL: default) */
+  const char *dform;       /* same for FP64 ("plain", "ozaki:8", ...) */
+} mublis_b200_server_config_t;
+
+typedef struct {
+  unsigned long long completed, batches, batched_requests, queue_depth;
+  double p50_latency_s, p99_latency_s, mean_latency_s;
+  double tflops;    /* completed flops / (last completion - first submission) */
+  double elapsed_s;
+  size_t hbm_in_use;
+} mublis_b200_server_stats_t;
+
+typedef struct mublis_b200_server mublis_b200_server_t;
+int mublis_b200_server_create(const mublis_b200_server_config_t *cfg, mublis_b200_server_t **srv);
+int mublis_b200_server_destroy(mublis_b200_server_t *srv);
+/* Route this process's device-resident calls through srv (NULL detaches). */
+int mublis_b200_server_attach(mublis_b200_server_t *srv);
+/* Operand handles: device memory counted against the server's HBM budget
+ * (status 3 when it would be exceeded). */
+int mublis_b200_server_alloc(mublis_b200_server_t *srv, size_t bytes, void **device_ptr);
+int mublis_b200_server_free(mublis_b200_server_t *srv, void *device_ptr);
+int mublis_b200_server_stats(mublis_b200_server_t *srv, mublis_b200_server_stats_t *out);
+int mublis_b200_server_reset_stats(mublis_b200_server_t *srv);
 
 /* SGEMM that allocates no memory.  No counterpart in the reference (its
  * CPU library draws packing buffers from a host pool, frame/base/pool.c).

@@ -52,6 +52,41 @@ class Product(ctypes.Structure):
 
 _I, _P, _L, _U32 = ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_uint32
 
+
+class GemmProblem(ctypes.Structure):
+    """mublis_b200_gemm_problem_t (include/mublis_b200.h)."""
+    _fields_ = [("trans_a", ctypes.c_int), ("trans_b", ctypes.c_int), ("m", ctypes.c_int),
+                ("n", ctypes.c_int), ("k", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double), ("a", ctypes.c_void_p), ("lda", ctypes.c_int),
+                ("b", ctypes.c_void_p), ("ldb", ctypes.c_int), ("c", ctypes.c_void_p),
+                ("ldc", ctypes.c_int)]
+
+
+class TrsmProblem(ctypes.Structure):
+    """mublis_b200_trsm_problem_t."""
+    _fields_ = [("uplo", ctypes.c_int), ("trans_a", ctypes.c_int), ("diag", ctypes.c_int),
+                ("m", ctypes.c_int), ("n", ctypes.c_int), ("alpha", ctypes.c_double),
+                ("a", ctypes.c_void_p), ("lda", ctypes.c_int), ("b", ctypes.c_void_p),
+                ("ldb", ctypes.c_int)]
+
+
+class ServerConfig(ctypes.Structure):
+    """mublis_b200_server_config_t."""
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("streams", ctypes.c_int),
+                ("batch_window_us", ctypes.c_int), ("small_max_dim", ctypes.c_int),
+                ("max_batch", ctypes.c_int), ("sform", ctypes.c_char_p),
+                ("dform", ctypes.c_char_p)]
+
+
+class ServerStats(ctypes.Structure):
+    """mublis_b200_server_stats_t."""
+    _fields_ = [("completed", ctypes.c_ulonglong), ("batches", ctypes.c_ulonglong),
+                ("batched_requests", ctypes.c_ulonglong), ("queue_depth", ctypes.c_ulonglong),
+                ("p50_latency_s", ctypes.c_double), ("p99_latency_s", ctypes.c_double),
+                ("mean_latency_s", ctypes.c_double), ("tflops", ctypes.c_double),
+                ("elapsed_s", ctypes.c_double), ("hbm_in_use", ctypes.c_size_t)]
+
+
 # "scalar" is replaced by c_float / c_double per precision.
 CBLAS_SIGNATURES = {
     "gemm": [_I, _I, _I, _I, _I, _I, "scalar", _P, _I, _P, _I, "scalar", _P, _I],
@@ -86,6 +121,23 @@ EXTENSIONS = {
     "mublis_b200_fill_s": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_b200_fill_d": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_get_context": ([_P], _I),
+    "mublis_b200_gemm_grouped": ([ctypes.c_char, ctypes.POINTER(GemmProblem), _I], _I),
+    "mublis_b200_trsm_grouped": ([ctypes.c_char, ctypes.POINTER(TrsmProblem), _I], _I),
+    "mublis_b200_plan_gemm_grouped": ([ctypes.c_char, ctypes.POINTER(GemmProblem), _I,
+                                       ctypes.POINTER(_P)], _I),
+    "mublis_b200_plan_trsm_grouped": ([ctypes.c_char, ctypes.POINTER(TrsmProblem), _I,
+                                       ctypes.POINTER(_P)], _I),
+    "mublis_b200_plan_run": ([_P], _I),
+    "mublis_b200_plan_destroy": ([_P], _I),
+    "mublis_b200_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)], _I),
+    "mublis_b200_server_destroy": ([_P], _I),
+    "mublis_b200_server_attach": ([_P], _I),
+    "mublis_b200_server_alloc": ([_P, ctypes.c_size_t, ctypes.POINTER(_P)], _I),
+    "mublis_b200_server_free": ([_P, _P], _I),
+    "mublis_b200_server_stats": ([_P, ctypes.POINTER(ServerStats)], _I),
+    "mublis_b200_server_reset_stats": ([_P], _I),
+    "mublis_b200_sgemm_noalloc": ([_I, _I, _I, _I, _I, ctypes.c_float, _P, _I, _I, _P, _I, _I,
+                                   ctypes.c_float, _P, _I, _I], _I),
 }
 
 SCALARS = {"s": ctypes.c_float, "d": ctypes.c_double}

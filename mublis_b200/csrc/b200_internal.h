@@ -35,7 +35,7 @@ enum { B200_F32 = 0, B200_F64 = 1 };
  * split, six products.  OZAKI: FP64 via int8 slices with exact int32
  * accumulation (slice count in b200_form_t.slices). */
 enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM_BF16X6 = 2,
-       B200_FORM_OZAKI = 3 };
+       B200_FORM_OZAKI = 3, B200_FORM_POLICY = 4 /* "auto": per-call size crossover */ };
 
 /* One product C(ji) := alpha * sum_t A_t B_t + beta * C over the domain of
  * `product`.  npairs is 1, or 2 for SYR2K (both pairs share the product's
@@ -104,6 +104,28 @@ int b200_l3_run(const b200_l3_desc_t *d);
 int b200_trsm_run(const b200_trsm_desc_t *d);
 int b200_scale_strided(int dtype, int m, int n, double beta, void *c, long rs, long cs,
                        mublis_l3_relation_t ji);
+
+/* grouped.cu: asynchronous batched execution on `stream` (the request
+ * server's coalesced launches).  Every descriptor must be batchable: a
+ * plain GEMM (general operands, domain ALL, one pair) of the given dtype, or
+ * a left TRSM of order <= 256 with alpha != 0. */
+int b200_l3_is_plain_gemm(const b200_l3_desc_t *d);
+int b200_grouped_gemm_async(int dtype, const b200_l3_desc_t *const *descs, int count,
+                            void *stream);
+int b200_grouped_trsm_async(int dtype, const b200_trsm_desc_t *const *descs, int count,
+                            void *stream);
+/* One plain GEMM read directly from its operands (no pack pass, no scratch),
+ * on the calling thread's stream. */
+int b200_gemm_direct(const b200_l3_desc_t *d);
+/* Same, with tiles at least min_rows tall (for in-place products). */
+int b200_gemm_direct_min_rows(const b200_l3_desc_t *d, int min_rows);
+
+/* serve.cu: when a request server is attached, the host front routes calls
+ * whose operands are all device-resident through it (blocking until done).
+ * b200_serve_attached() is 0 when none is attached. */
+int b200_serve_attached(void);
+int b200_serve_l3(const b200_l3_desc_t *d);
+int b200_serve_trsm(const b200_trsm_desc_t *d);
 
 /* ukr.cu: one MR x NR micro-tile on the device (packed host panels). */
 int b200_ukr_gemm(int dtype, int k, const void *alpha, const void *a, const void *b,

@@ -28,7 +28,7 @@ struct GemmEntry {
   const void *b;
   long rs_b, cs_b;  // element (p, j) of op(B) at b[p*rs_b + j*cs_b]
   void *c;
-  long ldc;
+  long rs_c, cs_c;  // element (i, j) of C at c[i*rs_c + j*cs_c]
   int tile0;        // first global tile index of this problem
   int tiles_m;
 };
@@ -39,9 +39,13 @@ struct GemmEntry {
 // covers (16*TM) x (16*TN).  Double-buffered shared memory with register
 // prefetch of the next k-block; loads follow whichever operand stride is 1.
 
+// `table` may be null: then the single problem `one` (passed by value in the
+// launch parameters) is the whole group -- the direct path for one small GEMM,
+// with no table upload.
 template <typename T, int TM, int TN>
 __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__restrict__ table,
-                                                           int nprob, int total_tiles) {
+                                                           int nprob, int total_tiles,
+                                                           const __grid_constant__ GemmEntry one) {
   constexpr int BM = 16 * TM, BN = 16 * TN, BK = sizeof(T) == 8 ? 8 : 16;
   constexpr int A_PER = BM * BK / 256, B_PER = BK * BN / 256;
   __shared__ __align__(16) T As[2][BK][BM];
@@ -51,11 +55,11 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
     // problem of this tile: last entry with tile0 <= tile
     int lo = 0, hi = nprob - 1;
-    while (lo < hi) {
+    while (table && lo < hi) {
       int mid = (lo + hi + 1) >> 1;
       if (table[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
     }
-    const GemmEntry &e = table[lo];
+    const GemmEntry &e = table ? table[lo] : one;
     const int local = tile - e.tile0;
     const long m0 = (long)(local % e.tiles_m) * BM, n0 = (long)(local / e.tiles_m) * BN;
     const T *A = (const T *)e.a, *B = (const T *)e.b;
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
       for (int j = 0; j < TN; ++j) {
         const long gj = n0 + tx + 16 * j;
         if (gj >= e.n) continue;
-        T *cij = Cm + gi + gj * e.ldc;
+        T *cij = Cm + gi * e.rs_c + gj * e.cs_c;
         T v = alpha * acc[i][j];
         if (beta != T(0)) v = fma(beta, *cij, v);
         *cij = v;
@@ -158,7 +162,7 @@ struct TrsmEntry {
   const void *a;
   long rs_a, cs_a;     // op(A) element (i, p) at a[i*rs_a + p*cs_a]
   void *b;
-  long ldb;
+  long rs_b, cs_b;     // element (i, j) of B at b[i*rs_b + j*cs_b]
   int lower, unit;
   int slab0;           // first global slab index
 };
@@ -189,7 +193,7 @@ __global__ void __launch_bounds__(256) grouped_trsm_kernel(const TrsmEntry *__re
     __syncthreads();
     for (int idx = tid; idx < m * TRSM_SLAB; idx += 256) {
       int i = idx % m, j = idx / m;
-      X[i][j] = j < ncol ? alpha * Bm[i + (j0 + j) * e.ldb] : T(0);
+      X[i][j] = j < ncol ? alpha * Bm[i * e.rs_b + (j0 + j) * e.cs_b] : T(0);
     }
     __syncthreads();
     const int nblk = (m + 31) / 32;
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(256) grouped_trsm_kernel(const TrsmEntry *__re
     }
     for (int idx = tid; idx < m * TRSM_SLAB; idx += 256) {
       int i = idx % m, j = idx / m;
-      if (j < ncol) Bm[i + (j0 + j) * e.ldb] = X[i][j];
+      if (j < ncol) Bm[i * e.rs_b + (j0 + j) * e.cs_b] = X[i][j];
     }
   }
 }
@@ -259,15 +263,18 @@ int sm_count() {
 
 template <typename T>
 int launch_gemm_variant(int variant, const GemmEntry *dtable, int nprob, int tiles,
-                        cudaStream_t s) {
+                        cudaStream_t s, const GemmEntry *one = nullptr) {
   if (tiles <= 0) return B200_OK;
   const int grid = std::min(tiles, sm_count() * 4);
-  B200ProfScope prof(sizeof(T) == 4 ? "grouped_sgemm" : "grouped_dgemm", s);
+  GemmEntry single;
+  if (one) single = *one; else memset(&single, 0, sizeof single);
+  B200ProfScope prof(one ? (sizeof(T) == 4 ? "direct_sgemm" : "direct_dgemm")
+                         : (sizeof(T) == 4 ? "grouped_sgemm" : "grouped_dgemm"), s);
   switch (variant) {
-  case TILE_32: grouped_gemm_kernel<T, 2, 2><<<grid, 256, 0, s>>>(dtable, nprob, tiles); break;
-  case TILE_64: grouped_gemm_kernel<T, 4, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles); break;
-  case TILE_128x64: grouped_gemm_kernel<T, 8, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles); break;
-  default: grouped_gemm_kernel<T, 8, 8><<<grid, 256, 0, s>>>(dtable, nprob, tiles); break;
+  case TILE_32: grouped_gemm_kernel<T, 2, 2><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  case TILE_64: grouped_gemm_kernel<T, 4, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  case TILE_128x64: grouped_gemm_kernel<T, 8, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  default: grouped_gemm_kernel<T, 8, 8><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
   }
   B200_LAUNCH_CHECK();
   return B200_OK;
@@ -329,7 +336,8 @@ int to_entries(char dtype, const mublis_b200_gemm_problem_t *p, int count,
     e.rs_b = x.trans_b == MUBLIS_TRANSPOSE ? x.ldb : 1;
     e.cs_b = x.trans_b == MUBLIS_TRANSPOSE ? 1 : x.ldb;
     e.c = x.c;
-    e.ldc = x.ldc;
+    e.rs_c = 1;
+    e.cs_c = x.ldc;
     cls[size_class(x.m, x.n)].push_back(e);
   }
   (void)dtype;
@@ -432,7 +440,8 @@ int to_trsm(const mublis_b200_trsm_problem_t *p, int count, TrsmGroup &g, cudaSt
     e.lower = (x.uplo == MUBLIS_LOWER) != tr;
     e.unit = x.diag == MUBLIS_UNIT_DIAG;
     e.b = x.b;
-    e.ldb = x.ldb;
+    e.rs_b = 1;
+    e.cs_b = x.ldb;
     e.slab0 = slabs;
     slabs += (int)b200_ceil_div(x.n, TRSM_SLAB);
     g.entries.push_back(e);
@@ -534,6 +543,151 @@ int capture(mublis_b200_plan *pl) {
 }
 
 }  // namespace
+
+// ---- descriptor-based asynchronous entry points (the request server) --------
+
+extern "C" int b200_l3_is_plain_gemm(const b200_l3_desc_t *d) {
+  const mublis_l3_product_t &p = d->product;
+  return d->npairs == 1 && p.domain.jp == MUBLIS_L3_ALL && p.domain.ji == MUBLIS_L3_ALL &&
+         p.domain.pi == MUBLIS_L3_ALL && p.a.struc == MUBLIS_STRUC_GENERAL &&
+         p.b.struc == MUBLIS_STRUC_GENERAL;
+}
+
+extern "C" int b200_grouped_gemm_async(int dtype, const b200_l3_desc_t *const *descs, int count,
+                                       void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<GemmEntry> cls[NCLASS];
+  for (int q = 0; q < count; ++q) {
+    const b200_l3_desc_t &d = *descs[q];
+    if (d.m <= 0 || d.n <= 0) continue;
+    if (!b200_l3_is_plain_gemm(&d) || d.dtype != dtype)
+      return b200_set_error(B200_EINVAL, "grouped: not a plain GEMM of this precision");
+    GemmEntry e;
+    memset(&e, 0, sizeof e);
+    e.m = d.m;
+    e.n = d.n;
+    e.k = d.alpha != 0.0 ? d.k : 0;
+    e.alpha = d.alpha;
+    e.beta = d.beta;
+    e.a = d.a[0];
+    e.rs_a = d.rs_a[0];
+    e.cs_a = d.cs_a[0];
+    e.b = d.b[0];
+    e.rs_b = d.rs_b[0];
+    e.cs_b = d.cs_b[0];
+    e.c = d.c;
+    e.rs_c = d.rs_c;
+    e.cs_c = d.cs_c;
+    cls[size_class(d.m, d.n)].push_back(e);
+  }
+  GemmGroup g[NCLASS];
+  int st = B200_OK;
+  for (int c = 0; c < NCLASS && st == B200_OK; ++c) {
+    if (cls[c].empty()) continue;
+    int bucket = 31 - __builtin_clz((unsigned)cls[c].size());
+    int v;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      v = g_tuned[dtype == B200_F64][c][bucket] ? g_tuned[dtype == B200_F64][c][bucket] - 1
+                                                : kDefaultVariant[c];
+    }
+    g[c].entries = cls[c];
+    g[c].variant = v;
+    int t = 0;
+    for (auto &e : g[c].entries) {
+      e.tile0 = t;
+      e.tiles_m = (int)b200_ceil_div(e.m, kTileBM[v]);
+      t += e.tiles_m * (int)b200_ceil_div(e.n, kTileBN[v]);
+    }
+    g[c].tiles = t;
+    if (cudaMallocAsync((void **)&g[c].dtable, sizeof(GemmEntry) * g[c].entries.size(), s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(g[c].dtable, g[c].entries.data(), sizeof(GemmEntry) * g[c].entries.size(),
+                        cudaMemcpyHostToDevice, s) != cudaSuccess)
+      st = b200_set_error(B200_ECUDA, "grouped: table upload failed");
+  }
+  if (st == B200_OK)
+    st = dtype == B200_F64 ? run_groups<double>(g, s) : run_groups<float>(g, s);
+  for (auto &x : g)
+    if (x.dtable) cudaFreeAsync(x.dtable, s);
+  return st;
+}
+
+// One small plain GEMM without packing: the grouped kernel with the problem
+// in its launch parameters (used by the TRSM recursion for thin updates).
+extern "C" int b200_gemm_direct_min_rows(const b200_l3_desc_t *d, int min_rows);
+
+extern "C" int b200_gemm_direct(const b200_l3_desc_t *d) { return b200_gemm_direct_min_rows(d, 0); }
+
+// min_rows: smallest tile height allowed (an in-place product needs a tile
+// to cover all rows of the block it overwrites).
+extern "C" int b200_gemm_direct_min_rows(const b200_l3_desc_t *d, int min_rows) {
+  if (d->m <= 0 || d->n <= 0) return B200_OK;
+  if (!b200_l3_is_plain_gemm(d)) return b200_set_error(B200_EINVAL, "direct gemm: not plain");
+  GemmEntry e;
+  memset(&e, 0, sizeof e);
+  e.m = d->m;
+  e.n = d->n;
+  e.k = d->alpha != 0.0 ? d->k : 0;
+  e.alpha = d->alpha;
+  e.beta = d->beta;
+  e.a = d->a[0];
+  e.rs_a = d->rs_a[0];
+  e.cs_a = d->cs_a[0];
+  e.b = d->b[0];
+  e.rs_b = d->rs_b[0];
+  e.cs_b = d->cs_b[0];
+  e.c = d->c;
+  e.rs_c = d->rs_c;
+  e.cs_c = d->cs_c;
+  int v = std::max(d->m, d->n) <= 64 ? TILE_32 : (std::min(d->m, d->n) <= 128 ? TILE_64 : TILE_128);
+  while (kTileBM[v] < min_rows && v < TILE_128) ++v;
+  if (kTileBM[v] < min_rows) return b200_set_error(B200_EINVAL, "direct gemm: tile too short");
+  e.tile0 = 0;
+  e.tiles_m = (int)b200_ceil_div(e.m, kTileBM[v]);
+  const int tiles = e.tiles_m * (int)b200_ceil_div(e.n, kTileBN[v]);
+  cudaStream_t s = b200_cur_stream();
+  return d->dtype == B200_F64 ? launch_gemm_variant<double>(v, nullptr, 1, tiles, s, &e)
+                              : launch_gemm_variant<float>(v, nullptr, 1, tiles, s, &e);
+}
+
+extern "C" int b200_grouped_trsm_async(int dtype, const b200_trsm_desc_t *const *descs, int count,
+                                       void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  TrsmGroup g;
+  int slabs = 0;
+  for (int q = 0; q < count; ++q) {
+    const b200_trsm_desc_t &d = *descs[q];
+    if (d.m <= 0 || d.n <= 0) continue;
+    if (d.m > TRSM_MAX_ORDER || d.dtype != dtype || d.alpha == 0.0)
+      return b200_set_error(B200_EINVAL, "grouped: TRSM not batchable");
+    TrsmEntry e;
+    memset(&e, 0, sizeof e);
+    e.m = d.m;
+    e.n = d.n;
+    e.alpha = d.alpha;
+    e.a = d.a;
+    e.rs_a = d.rs_a;
+    e.cs_a = d.cs_a;
+    e.lower = d.uplo == MUBLIS_LOWER;
+    e.unit = d.unit_diag != 0;
+    e.b = d.b;
+    e.rs_b = d.rs_b;
+    e.cs_b = d.cs_b;
+    e.slab0 = slabs;
+    slabs += (int)b200_ceil_div(d.n, TRSM_SLAB);
+    g.entries.push_back(e);
+  }
+  g.slabs = slabs;
+  if (g.entries.empty()) return B200_OK;
+  if (cudaMallocAsync((void **)&g.dtable, sizeof(TrsmEntry) * g.entries.size(), s) != cudaSuccess ||
+      cudaMemcpyAsync(g.dtable, g.entries.data(), sizeof(TrsmEntry) * g.entries.size(),
+                      cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return b200_set_error(B200_ECUDA, "grouped: table upload failed");
+  int st = dtype == B200_F64 ? launch_trsm_group<double>(g, s) : launch_trsm_group<float>(g, s);
+  cudaFreeAsync(g.dtable, s);
+  return st;
+}
 
 extern "C" {
 

@@ -125,7 +125,9 @@ int b200_front_l3(b200_l3_desc_t *d) {
     dd.rs_c = v.rs;
     dd.cs_c = v.cs;
   }
-  if (st == B200_OK) st = b200_l3_run(&dd);
+  /* Device-resident calls go through the request server when one is
+   * attached (continuous batching across calling threads). */
+  if (st == B200_OK) st = ss.n == 0 && b200_serve_attached() ? b200_serve_l3(&dd) : b200_l3_run(&dd);
   return b200_stage_end(&ss, st);
 }
 
@@ -194,7 +196,7 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   d.c = vb.ptr;
   d.rs_c = vb.rs;
   d.cs_c = vb.cs;
-  st = b200_l3_run(&d);
+  st = ss.n == 0 && b200_serve_attached() ? b200_serve_l3(&d) : b200_l3_run(&d);
   return b200_stage_end(&ss, st);
 }
 
@@ -242,7 +244,7 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   d.uplo = uplo;
   d.unit_diag = diag == MUBLIS_UNIT_DIAG;
   d.form = B200_FORM_AUTO;
-  st = b200_trsm_run(&d);
+  st = ss.n == 0 && b200_serve_attached() ? b200_serve_trsm(&d) : b200_trsm_run(&d);
   return b200_stage_end(&ss, st);
 }
 

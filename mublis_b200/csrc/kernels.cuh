@@ -88,9 +88,3 @@ int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s);
 
 template <typename T>
 int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStream_t s);
-
-// Diagonal-block solve of a left TRSM: rows [0, mb) of B (mb <= 64) solved
-// against the mb x mb triangle at a (op applied via strides), in place.
-template <typename T>
-int launch_trsm_leaf(int mb, int n, const T *a, long rs_a, long cs_a, T *b, long rs_b, long cs_b,
-                     bool lower, bool unit, cudaStream_t s);

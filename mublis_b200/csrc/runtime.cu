@@ -46,6 +46,7 @@ int parse_form(const char *s, int *slices) {
   if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
   if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
   if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
+  if (!strcmp(s, "auto")) return B200_FORM_POLICY;
   if (!strncmp(s, "ozaki", 5)) {
     if (s[5] == ':' && slices) *slices = atoi(s + 6);
     return B200_FORM_OZAKI;
@@ -79,9 +80,11 @@ void do_init() {
   int slices = 0;
   int sf = parse_form(getenv("MUBLIS_B200_SFORM"), nullptr);
   int df = parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
-  if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6)
+  if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6 ||
+      sf == B200_FORM_POLICY)
     g_default_form[B200_F32] = sf;
-  if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI) g_default_form[B200_F64] = df;
+  if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI || df == B200_FORM_POLICY)
+    g_default_form[B200_F64] = df;
   if (slices > 0) g_default_slices = slices;
   g_init_status = B200_OK;
 }
@@ -182,9 +185,10 @@ int b200_get_default_slices(void) { return g_default_slices; }
 
 int b200_set_default_form(int dtype, int form, int slices) {
   if (dtype == B200_F32 && form != B200_FORM_PLAIN && form != B200_FORM_BF16X3 &&
-      form != B200_FORM_BF16X6)
+      form != B200_FORM_BF16X6 && form != B200_FORM_POLICY)
     return B200_EINVAL;
-  if (dtype == B200_F64 && form != B200_FORM_PLAIN && form != B200_FORM_OZAKI)
+  if (dtype == B200_F64 && form != B200_FORM_PLAIN && form != B200_FORM_OZAKI &&
+      form != B200_FORM_POLICY)
     return B200_EINVAL;
   g_default_form[dtype == B200_F64] = form;
   if (slices > 0) g_default_slices = slices;

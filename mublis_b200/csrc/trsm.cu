@@ -8,10 +8,14 @@
 //   * recursive halving: solve the top half, update the bottom half with one
 //     GEMM (k = half the order, so it runs at GEMM speed), solve the bottom
 //     half (upper: mirror image);
-//   * leaves of at most 32 rows are solved by trsm_leaf_kernel: the leaf
-//     triangle sits in shared memory with the reciprocal diagonal (computed
-//     once, multiplied -- never divided -- as the reference does), each
-//     thread owns one right-hand-side column in registers;
+//   * leaves are the 64 x 64 diagonal blocks.  All of them are inverted up
+//     front in one launch (trsm_inv_diag_kernel: substitution against the
+//     reciprocal diagonal, computed once and multiplied -- never divided --
+//     as the reference does; the unstored triangle and a unit diagonal are
+//     never read), so each leaf solve is X_b = inv(A_bb) B_b, a parallel
+//     64 x n GEMM instead of a 64-deep dependent chain per column;
+//   * updates and leaf products with k <= 256 read their operands directly
+//     (no pack pass); larger ones use the packed driver path;
 //   * the unit diagonal and the unstored triangle are never read.
 // alpha is applied once up front (the reference's alpha_eff on the first
 // block, trsm.c:96-97).
@@ -21,96 +25,126 @@
 
 namespace {
 
-constexpr int LEAF = 32;
+constexpr int LEAF = 64;  // rows per diagonal block (leaf)
 
-template <typename T, int NB>
-__global__ void __launch_bounds__(128) trsm_leaf_kernel(int mb, int n, const T *a, long rs_a,
-                                                        long cs_a, T *b, long rs_b, long cs_b,
-                                                        bool lower, bool unit) {
-  __shared__ T L[NB][NB + 1];
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    int i = idx % NB, p = idx / NB;
+// One CTA per diagonal block: thread j computes column j of the inverse of
+// the block's (lower or upper) triangle by substitution, L x = e_j.  Rows
+// past the matrix order are padded with the identity.  Output: block b as a
+// LEAF x LEAF column-major matrix at inv + b * LEAF * LEAF.
+template <typename T>
+__global__ void __launch_bounds__(LEAF) trsm_inv_diag_kernel(int m, const T *a, long rs_a,
+                                                              long cs_a, bool lower, bool unit,
+                                                              T *inv) {
+  __shared__ T L[LEAF][LEAF + 1];
+  const int b = blockIdx.x, j = threadIdx.x;
+  const long r0 = (long)b * LEAF;
+  const int mb = (int)min((long)LEAF, m - r0);
+  const bool rows_fast = labs(rs_a) <= labs(cs_a);
+  for (int idx = j; idx < LEAF * LEAF; idx += LEAF) {
+    int i = rows_fast ? idx % LEAF : idx / LEAF, p = rows_fast ? idx / LEAF : idx % LEAF;
     T v = T(0);
     if (i < mb && p < mb) {
-      if (i == p) v = unit ? T(1) : T(1) / a[i * rs_a + i * cs_a];
-      else if (lower ? p < i : p > i) v = a[i * rs_a + p * cs_a];
+      if (i == p) v = unit ? T(1) : T(1) / a[(r0 + i) * rs_a + (r0 + i) * cs_a];
+      else if (lower ? p < i : p > i) v = a[(r0 + i) * rs_a + (r0 + p) * cs_a];
+    } else if (i == p) {
+      v = T(1);
     }
     L[i][p] = v;
   }
   __syncthreads();
-  const long j = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  T x[NB];
+  T x[LEAF];
 #pragma unroll
-  for (int i = 0; i < NB; ++i) x[i] = i < mb ? b[i * rs_b + j * cs_b] : T(0);
+  for (int i = 0; i < LEAF; ++i) x[i] = T(0);
   if (lower) {
 #pragma unroll
-    for (int i = 0; i < NB; ++i) {
-      T r = x[i];
+    for (int i = 0; i < LEAF; ++i) {
+      T r = i == j ? T(1) : T(0);
 #pragma unroll
       for (int p = 0; p < i; ++p) r = fma(-L[i][p], x[p], r);
       x[i] = r * L[i][i];
     }
   } else {
 #pragma unroll
-    for (int i = NB - 1; i >= 0; --i) {
-      T r = x[i];
+    for (int i = LEAF - 1; i >= 0; --i) {
+      T r = i == j ? T(1) : T(0);
 #pragma unroll
-      for (int p = i + 1; p < NB; ++p) r = fma(-L[i][p], x[p], r);
+      for (int p = i + 1; p < LEAF; ++p) r = fma(-L[i][p], x[p], r);
       x[i] = r * L[i][i];
     }
   }
+  T *out = inv + (size_t)b * LEAF * LEAF + (size_t)j * LEAF;
 #pragma unroll
-  for (int i = 0; i < NB; ++i)
-    if (i < mb) b[i * rs_b + j * cs_b] = x[i];
+  for (int i = 0; i < LEAF; ++i) out[i] = x[i];
 }
 
-}  // namespace
-
 template <typename T>
-int launch_trsm_leaf(int mb, int n, const T *a, long rs_a, long cs_a, T *b, long rs_b, long cs_b,
-                     bool lower, bool unit, cudaStream_t s) {
-  if (mb <= 0 || n <= 0) return B200_OK;
-  if (mb > LEAF) return b200_set_error(B200_EINVAL, "trsm leaf larger than 32");
-  B200ProfScope prof(sizeof(T) == 4 ? "trsm_leaf_s" : "trsm_leaf_d", s);
-  trsm_leaf_kernel<T, LEAF><<<(unsigned)b200_ceil_div(n, 128), 128, 0, s>>>(
-      mb, n, a, rs_a, cs_a, b, rs_b, cs_b, lower, unit);
+int launch_inv_diag(int m, const T *a, long rs_a, long cs_a, bool lower, bool unit, T *inv,
+                    cudaStream_t s) {
+  const int blocks = (int)b200_ceil_div(m, LEAF);
+  B200ProfScope prof(sizeof(T) == 4 ? "trsm_inv_s" : "trsm_inv_d", s);
+  trsm_inv_diag_kernel<T><<<blocks, LEAF, 0, s>>>(m, a, rs_a, cs_a, lower, unit, inv);
   B200_LAUNCH_CHECK();
   return B200_OK;
 }
 
-template int launch_trsm_leaf<float>(int, int, const float *, long, long, float *, long, long,
-                                     bool, bool, cudaStream_t);
-template int launch_trsm_leaf<double>(int, int, const double *, long, long, double *, long, long,
-                                      bool, bool, cudaStream_t);
+}  // namespace
 
 namespace {
 
+b200_l3_desc_t plain_gemm_desc(int dtype, int form, int slices) {
+  b200_l3_desc_t g;
+  memset(&g, 0, sizeof g);
+  g.dtype = dtype;
+  g.npairs = 1;
+  mublis_l3_operand_t gen = {MUBLIS_STRUC_GENERAL, MUBLIS_DENSE, MUBLIS_PACKM_DIAG_NONUNIT};
+  g.product.domain.jp = g.product.domain.ji = g.product.domain.pi = MUBLIS_L3_ALL;
+  g.product.a = gen;
+  g.product.b = gen;
+  g.form = form;
+  g.slices = slices;
+  return g;
+}
+
 template <typename T>
-int trsm_rec(const b200_trsm_desc_t *d, long r0, long r1) {
+int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   const T *a = (const T *)d->a;
   T *b = (T *)d->b;
   const bool lower = d->uplo == MUBLIS_LOWER;
   long rows = r1 - r0;
-  if (rows <= LEAF)
-    return launch_trsm_leaf<T>((int)rows, d->n, a + r0 * d->rs_a + r0 * d->cs_a, d->rs_a,
-                               d->cs_a, b + r0 * d->rs_b, d->rs_b, d->cs_b, lower,
-                               d->unit_diag != 0, b200_cur_stream());
+  if (rows <= LEAF) {
+    // X_b = inv(A_bb) B_b, in place: every CTA of the direct kernel covers
+    // all rows of the leaf for its columns (tile height >= LEAF), so it reads
+    // its B columns completely before it writes them, and CTAs own disjoint
+    // columns.
+    b200_l3_desc_t g = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
+    g.m = (int)rows;
+    g.n = d->n;
+    g.k = (int)rows;
+    g.alpha = 1.0;
+    g.beta = 0.0;
+    g.a[0] = inv + (r0 / LEAF) * LEAF * LEAF;
+    g.rs_a[0] = 1;
+    g.cs_a[0] = LEAF;
+    g.b[0] = b + r0 * d->rs_b;
+    g.rs_b[0] = d->rs_b;
+    g.cs_b[0] = d->cs_b;
+    g.c = b + r0 * d->rs_b;
+    g.rs_c = d->rs_b;
+    g.cs_c = d->cs_b;
+    return b200_gemm_direct_min_rows(&g, LEAF);
+  }
   long half = b200_round_up((rows + 1) / 2, LEAF);
   long mid = r0 + half;
   // Rows solved first (src) and rows updated by them (dst).
   long s0 = lower ? r0 : mid, s1 = lower ? mid : r1;
   long t0 = lower ? mid : r0, t1 = lower ? r1 : mid;
-  B200_TRY(trsm_rec<T>(d, s0, s1));
-  b200_l3_desc_t g;
-  memset(&g, 0, sizeof g);
-  g.dtype = d->dtype;
+  B200_TRY(trsm_rec<T>(d, inv, s0, s1));
+  b200_l3_desc_t g = plain_gemm_desc(d->dtype, d->form, d->slices);
   g.m = (int)(t1 - t0);
   g.n = d->n;
   g.k = (int)(s1 - s0);
   g.alpha = -1.0;
   g.beta = 1.0;
-  g.npairs = 1;
   g.a[0] = a + t0 * d->rs_a + s0 * d->cs_a;
   g.rs_a[0] = d->rs_a;
   g.cs_a[0] = d->cs_a;
@@ -120,14 +154,23 @@ int trsm_rec(const b200_trsm_desc_t *d, long r0, long r1) {
   g.c = b + t0 * d->rs_b;
   g.rs_c = d->rs_b;
   g.cs_c = d->cs_b;
-  mublis_l3_operand_t gen = {MUBLIS_STRUC_GENERAL, MUBLIS_DENSE, MUBLIS_PACKM_DIAG_NONUNIT};
-  g.product.domain.jp = g.product.domain.ji = g.product.domain.pi = MUBLIS_L3_ALL;
-  g.product.a = gen;
-  g.product.b = gen;
-  g.form = d->form;
-  g.slices = d->slices;
-  B200_TRY(b200_l3_run(&g));
-  return trsm_rec<T>(d, t0, t1);
+  // Thin updates (small k) read their operands directly; thick ones go
+  // through the packed driver path (and the tensor-core forms).
+  B200_TRY(g.k <= 256 ? b200_gemm_direct(&g) : b200_l3_run(&g));
+  return trsm_rec<T>(d, inv, t0, t1);
+}
+
+template <typename T>
+int trsm_solve(const b200_trsm_desc_t *d) {
+  cudaStream_t s = b200_cur_stream();
+  T *inv = nullptr;
+  const long blocks = b200_ceil_div(d->m, LEAF);
+  B200_TRY(b200_alloc((void **)&inv, sizeof(T) * blocks * LEAF * LEAF));
+  int st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
+                              d->unit_diag != 0, inv, s);
+  if (st == B200_OK) st = trsm_rec<T>(d, inv, 0, d->m);
+  b200_free(inv);
+  return st;
 }
 
 }  // namespace
@@ -139,6 +182,6 @@ extern "C" int b200_trsm_run(const b200_trsm_desc_t *d) {
   if (d->alpha != 1.0)
     B200_TRY(b200_scale_strided(d->dtype, d->m, d->n, d->alpha, d->b, d->rs_b, d->cs_b,
                                 MUBLIS_L3_ALL));
-  if (d->dtype == B200_F32) return trsm_rec<float>(d, 0, d->m);
-  return trsm_rec<double>(d, 0, d->m);
+  if (d->dtype == B200_F32) return trsm_solve<float>(d);
+  return trsm_solve<double>(d);
 }

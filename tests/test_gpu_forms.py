@@ -1,0 +1,167 @@
+"""Precision forms on the tensor cores, against the oracle.
+
+Stated tolerances (normwise relative error against the long-double oracle
+restatement, or against a double-double evaluation of sampled entries at
+8192^3):
+  plain FP32 / FP64     4 * k * u                      (u = 2^-24 / 2^-53)
+  bf16x6 (FP32)         4 * k * 2^-24                  (same as plain)
+  bf16x3 (FP32)         2^-15   (16-bit split of each input: ~2^-17 per
+                                 element, not k-dependent)
+  ozaki:8 (FP64)        4 * k * 2^-53                  (same as plain)
+  ozaki:7 (FP64)        2^-44
+The 8192^3 study also checks the headline claims: bf16x6 has the error of
+plain FP32 (within 1.5x) and ozaki:8 has at most the error of plain FP64.
+Run with -s to print the measured table.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import mublis_b200 as mb
+from oracle import oracle as orc
+from tests import cases as cs
+
+pytestmark = pytest.mark.gpu
+
+TOL = {
+    "plain": lambda k, u: 4 * k * u,
+    "bf16x6": lambda k, u: 4 * k * 2.0 ** -24,
+    "bf16x3": lambda k, u: 2.0 ** -15,
+    "ozaki:8": lambda k, u: 4 * k * 2.0 ** -53,
+    "ozaki:7": lambda k, u: 2.0 ** -44,
+}
+
+
+@pytest.fixture(scope="module")
+def lib():
+    lib = mb.load()
+    assert lib.mublis_b200_init() == 0, mb.last_error(lib)
+    orc.set_threads(16)
+    yield lib
+    lib.mublis_b200_set_form(b"s", b"plain")
+    lib.mublis_b200_set_form(b"d", b"plain")
+
+
+def run(lib, case, form):
+    p = b"s" if case["dtype"] == "float32" else b"d"
+    assert lib.mublis_b200_set_form(p, form.encode()) == 0
+    a, b, c0 = cs.build(case)
+    out = c0.copy(order="K")
+    cs.cblas_call(lib, case, a, b, out)
+    ref = c0.copy(order="K")
+    cs.oracle_call(case, a, b, ref)
+    lib.mublis_b200_set_form(p, b"plain")
+    return cs.normwise_error(case, out, ref, a, b, c0), np.isfinite(out[cs.active_mask(case)]).all()
+
+
+FAMILY = [("gemm", dict(ta=False, tb=False)), ("gemm", dict(ta=True, tb=True)),
+          ("symm", dict(right=False, lower=True)), ("symm", dict(right=True, lower=False)),
+          ("syrk", dict(ta=False, lower=True)), ("syr2k", dict(ta=True, lower=False)),
+          ("trmm", dict(right=False, lower=True, ta=False, unit=False)),
+          ("trmm", dict(right=True, lower=False, ta=True, unit=True)),
+          ("trsm", dict(right=False, lower=True, ta=False, unit=False))]
+
+
+@pytest.mark.parametrize("form", ["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("routine,flags", FAMILY, ids=[f"{r}{i}" for i, (r, _) in enumerate(FAMILY)])
+def test_fp32_tensor_forms(lib, form, routine, flags):
+    case = dict(routine=routine, dtype="float32", order="F", m=640, n=544, k=704, alpha=0.75,
+                beta=0.25, seed=21, **flags)
+    if routine in ("syrk", "syr2k"):
+        case["m"] = case["n"]
+    err, finite = run(lib, case, form)
+    assert finite
+    assert err <= TOL[form](cs.inner_dim(case), 2.0 ** -24), err
+
+
+@pytest.mark.parametrize("form", ["ozaki:7", "ozaki:8"])
+@pytest.mark.parametrize("routine,flags", FAMILY, ids=[f"{r}{i}" for i, (r, _) in enumerate(FAMILY)])
+def test_fp64_ozaki(lib, form, routine, flags):
+    case = dict(routine=routine, dtype="float64", order="F", m=600, n=520, k=680, alpha=0.75,
+                beta=0.25, seed=22, **flags)
+    if routine in ("syrk", "syr2k"):
+        case["m"] = case["n"]
+    err, finite = run(lib, case, form)
+    assert finite
+    assert err <= TOL[form](cs.inner_dim(case), 2.0 ** -53), err
+
+
+def test_auto_form_matches_plain_error(lib):
+    case = dict(routine="gemm", dtype="float32", order="F", m=1024, n=1024, k=1024, ta=False,
+                tb=False, alpha=1.0, beta=0.5, seed=3)
+    err, finite = run(lib, case, "auto")
+    assert finite and err <= TOL["plain"](1024, 2.0 ** -24)
+
+
+def test_wide_range_inputs_ozaki(lib):
+    """The wide draw (|x| = m * 2^e, e in [-10, 10]) stresses the per-row
+    scaling of the Ozaki split."""
+    torch = pytest.importorskip("torch")
+    n = 1536
+    a = orc.fill(n, n, np.float64, 4, 0, orc.WIDE)
+    b = orc.fill(n, n, np.float64, 4, 1, orc.WIDE)
+    rows = np.random.default_rng(0).integers(0, n, 512)
+    cols = np.random.default_rng(1).integers(0, n, 512)
+    hi, lo = orc.dd_gemm_entries(a, b, rows, cols)
+    exact = hi + lo
+    den = np.linalg.norm(a) * np.linalg.norm(b)
+    errs = {}
+    for form in ("plain", "ozaki:8"):
+        assert lib.mublis_b200_set_form(b"d", form.encode()) == 0
+        c = np.zeros((n, n), order="F")
+        assert lib.mublis_dgemm(0, 0, n, n, n, 1.0, a.ctypes.data, 1, n, b.ctypes.data, 1, n,
+                                0.0, c.ctypes.data, 1, n) == 0
+        d = c[rows, cols] - exact
+        errs[form] = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
+    lib.mublis_b200_set_form(b"d", b"plain")
+    assert errs["ozaki:8"] <= max(errs["plain"], 4 * n * 2.0 ** -53), errs
+
+
+def _device_matrix(torch, lib, p, n, seed, mid, kind=0):
+    dt = torch.float32 if p == "s" else torch.float64
+    t = torch.empty(n, n, dtype=dt, device="cuda")
+    fill = getattr(lib, f"mublis_b200_fill_{p}")
+    assert fill(ctypes.c_void_p(t.data_ptr()), n, n, n, seed, mid, kind) == 0
+    return t
+
+
+@pytest.mark.parametrize("kind", [orc.UNIFORM, orc.WIDE], ids=["uniform", "wide"])
+def test_precision_study_8192(lib, kind):
+    """Config-3 study: m = n = k = 8192, uniform and wide draws; normwise and
+    max elementwise error of every form against double-double values of 1024
+    sampled entries of alpha*A*B + beta*C (alpha 1, beta 0.5)."""
+    torch = pytest.importorskip("torch")
+    n, ns = 8192, 1024
+    rng = np.random.default_rng(7)
+    rows, cols = rng.integers(0, n, ns), rng.integers(0, n, ns)
+    table = {}
+    for p, forms in (("s", ["plain", "bf16x3", "bf16x6"]), ("d", ["plain", "ozaki:7", "ozaki:8"])):
+        a, b, c0 = (_device_matrix(torch, lib, p, n, 0, i, kind) for i in range(3))
+        ah, bh, ch = (np.asfortranarray(x.cpu().numpy().T) for x in (a, b, c0))
+        hi, lo = orc.dd_gemm_entries(ah, bh, rows, cols, alpha=1.0, beta=0.5, c0=ch)
+        exact = hi + lo
+        den = (np.linalg.norm(ah.astype(np.float64)) * np.linalg.norm(bh.astype(np.float64)) +
+               0.5 * np.linalg.norm(ch.astype(np.float64)))
+        fn = getattr(lib, f"mublis_{p}gemm")
+        for form in forms:
+            assert lib.mublis_b200_set_form(p.encode(), form.encode()) == 0
+            c = c0.clone()
+            torch.cuda.synchronize()
+            assert fn(0, 0, n, n, n, 1.0, a.data_ptr(), 1, n, b.data_ptr(), 1, n, 0.5,
+                      c.data_ptr(), 1, n) == 0
+            got = c.cpu().numpy().T[rows, cols].astype(np.float64)
+            d = got - exact
+            nw = np.sqrt((d ** 2).sum() * (n * n / ns)) / den
+            mx = float(np.max(np.abs(d) / np.maximum(np.abs(exact), 1e-300)))
+            table[f"{p}gemm {form}"] = (nw, mx)
+        lib.mublis_b200_set_form(p.encode(), b"plain")
+        del a, b, c0
+        torch.cuda.empty_cache()
+    print(f"\nm=n=k=8192, draw={'wide' if kind else 'uniform'}: normwise, max elementwise rel")
+    for key, (nw, mx) in table.items():
+        print(f"  {key:14s} {nw:.3e}  {mx:.3e}")
+    assert table["sgemm bf16x6"][0] <= 1.5 * table["sgemm plain"][0]
+    assert table["dgemm ozaki:8"][0] <= table["dgemm plain"][0]
+    assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
+    assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)

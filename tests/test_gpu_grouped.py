@@ -17,34 +17,13 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 
-class GemmProblem(ctypes.Structure):
-    _fields_ = [("trans_a", ctypes.c_int), ("trans_b", ctypes.c_int), ("m", ctypes.c_int),
-                ("n", ctypes.c_int), ("k", ctypes.c_int), ("alpha", ctypes.c_double),
-                ("beta", ctypes.c_double), ("a", ctypes.c_void_p), ("lda", ctypes.c_int),
-                ("b", ctypes.c_void_p), ("ldb", ctypes.c_int), ("c", ctypes.c_void_p),
-                ("ldc", ctypes.c_int)]
-
-
-class TrsmProblem(ctypes.Structure):
-    _fields_ = [("uplo", ctypes.c_int), ("trans_a", ctypes.c_int), ("diag", ctypes.c_int),
-                ("m", ctypes.c_int), ("n", ctypes.c_int), ("alpha", ctypes.c_double),
-                ("a", ctypes.c_void_p), ("lda", ctypes.c_int), ("b", ctypes.c_void_p),
-                ("ldb", ctypes.c_int)]
+GemmProblem, TrsmProblem = mb.GemmProblem, mb.TrsmProblem
 
 
 @pytest.fixture(scope="module")
 def glib():
     lib = mb.load()
     assert lib.mublis_b200_init() == 0, mb.last_error(lib)
-    P = ctypes.POINTER
-    lib.mublis_b200_gemm_grouped.argtypes = [ctypes.c_char, P(GemmProblem), ctypes.c_int]
-    lib.mublis_b200_trsm_grouped.argtypes = [ctypes.c_char, P(TrsmProblem), ctypes.c_int]
-    lib.mublis_b200_plan_gemm_grouped.argtypes = [ctypes.c_char, P(GemmProblem), ctypes.c_int,
-                                                  P(ctypes.c_void_p)]
-    lib.mublis_b200_plan_trsm_grouped.argtypes = [ctypes.c_char, P(TrsmProblem), ctypes.c_int,
-                                                  P(ctypes.c_void_p)]
-    lib.mublis_b200_plan_run.argtypes = [ctypes.c_void_p]
-    lib.mublis_b200_plan_destroy.argtypes = [ctypes.c_void_p]
     for p in (b"s", b"d"):
         lib.mublis_b200_set_form(p, b"plain")
     return lib

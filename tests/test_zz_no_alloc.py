@@ -25,16 +25,10 @@ import mublis_b200 as mb
 
 pytestmark = pytest.mark.gpu
 
-_P, _I, _F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
-NOALLOC_SIG = [_I, _I, _I, _I, _I, _F, _P, _I, _I, _P, _I, _I, _F, _P, _I, _I]
-
-
 @pytest.fixture(scope="module")
 def lib():
     lib = mb.load()
     assert lib.mublis_b200_init() == 0, mb.last_error(lib)
-    lib.mublis_b200_sgemm_noalloc.argtypes = NOALLOC_SIG
-    lib.mublis_b200_sgemm_noalloc.restype = _I
     lib.mublis_b200_set_form(b"s", b"plain")
     return lib
 
