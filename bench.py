@@ -286,10 +286,10 @@ def timed(torch, fn, steps: int):
     return e0.elapsed_time(e1) / steps
 
 
-def forms_study(torch, lib) -> dict:
-    """Precision forms at m = n = k = 8192 (one call each, event-timed)."""
+def forms_study(torch, lib, n: int = 8192) -> dict:
+    """Precision forms at m = n = k = n (8192 by default; one call each,
+    event-timed)."""
     out = {}
-    n = 8192
     for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6"]),
                          ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8"])):
         fill = getattr(lib, f"mublis_b200_fill_{p}")
@@ -304,7 +304,7 @@ def forms_study(torch, lib) -> dict:
                               ctypes.c_void_p(c.data_ptr()), n)
             call()
             ms = timed(torch, call, 2)
-            out[f"{p}gemm_8192_{f}"] = round(2.0 * n ** 3 / ms / 1e9, 2)
+            out[f"{p}gemm_{n}_{f}"] = round(2.0 * n ** 3 / ms / 1e9, 2)
         lib.mublis_b200_set_form(p.encode(), b"plain")
         del a, b, c
         torch.cuda.empty_cache()
@@ -524,6 +524,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-studies", action="store_true",
                     help="skip the grouped (config 4) and served (config 5) studies")
+    ap.add_argument("--only-forms", action="store_true",
+                    help="run only the precision-form study (for profiler captures)")
+    ap.add_argument("--forms-n", type=int, default=8192)
     ap.add_argument("--only-timed", action="store_true",
                     help="warm-up + timed steps only (for profiler launch lists)")
     args = ap.parse_args()
@@ -552,6 +555,12 @@ def main():
         lib.mublis_b200_set_form(p, b"plain")
     stream = torch.cuda.current_stream()
     mb.check(lib.mublis_b200_set_stream(ctypes.c_void_p(stream.cuda_stream)), lib)
+
+    if args.only_forms:
+        if rank == 0:
+            print(json.dumps({"forms_tflops": forms_study(torch, lib, args.forms_n),
+                              "n": args.forms_n}))
+        return
 
     n = args.n
     fam = Family(torch, lib, n, device=True)
@@ -634,7 +643,7 @@ def main():
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
-        forms = forms_study(torch, lib)
+        forms = forms_study(torch, lib, args.forms_n)
     grouped = served = None
     if rank == 0 and world == 1 and not args.no_studies:
         grouped = grouped_study(torch, lib)

@@ -18,6 +18,8 @@
 // Epilogue: C = alpha*acc + beta*C, and beta == 0 never reads C
 // (:111-112, :224-225).  A tile with an empty k-range writes beta*C, which is
 // the reference's "no update" pass (:88-121).
+#include <cstdlib>
+
 #include "kernels.cuh"
 
 namespace {
@@ -182,37 +184,61 @@ __global__ void scale_kernel(int m, int n, T beta, T *c, long rs, long cs, int j
   }
 }
 
-template <typename T>
-struct SimtTraits;
-template <>
-struct SimtTraits<float> {
-  static constexpr int WARPS_M = 4, WARPS_N = 2, STAGES = 4, MINB = 2;
-};
-template <>
-struct SimtTraits<double> {
-  static constexpr int WARPS_M = 4, WARPS_N = 2, STAGES = 4, MINB = 2;
-};
-
-}  // namespace
-
-template <typename T>
-int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s) {
-  using C = SimtConfig<T>;
-  using R = SimtTraits<T>;
-  auto kern = simt_gemm_kernel<T, C::BM, C::BN, C::BK, R::WARPS_M, R::WARPS_N, R::STAGES, R::MINB>;
-  const size_t smem = (size_t)R::STAGES * C::BK * (C::BM + C::BN) * sizeof(T);
+// Tile configurations: (BM, BN, warps along M, warps along N, cp.async
+// stages, min CTAs per SM).  Packed panels are padded to 128 in M and N, so
+// every configuration reads the same panels.  Index 0 is the default; the
+// others are kept for tuning (MUBLIS_B200_SIMT_S / MUBLIS_B200_SIMT_D).
+template <typename T, int BM, int BN, int WM, int WN, int ST, int MINB>
+int launch_cfg(const SimtGemmArgs<T> &a, cudaStream_t s) {
+  constexpr int BK = SimtConfig<T>::BK;
+  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB>;
+  const size_t smem = (size_t)ST * BK * (BM + BN) * sizeof(T);
   static bool configured = false;
   if (!configured) {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = true;
   }
-  long tiles = b200_ceil_div(a.m, C::BM) * b200_ceil_div(a.n, C::BN);
+  long tiles = b200_ceil_div(a.m, BM) * b200_ceil_div(a.n, BN);
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "gemm: too many tiles");
   B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
   kern<<<(unsigned)tiles, 256, smem, s>>>(a);
   B200_LAUNCH_CHECK();
   return B200_OK;
+}
+
+int simt_variant(bool dbl) {
+  static int v[2] = {-1, -1};
+  if (v[dbl] < 0) {
+    const char *e = getenv(dbl ? "MUBLIS_B200_SIMT_D" : "MUBLIS_B200_SIMT_S");
+    v[dbl] = e ? atoi(e) : 0;
+  }
+  return v[dbl];
+}
+
+}  // namespace
+
+template <typename T>
+int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s);
+
+template <>
+int launch_simt_gemm<float>(const SimtGemmArgs<float> &a, cudaStream_t s) {
+  switch (simt_variant(false)) {
+  case 1: return launch_cfg<float, 128, 128, 2, 4, 4, 2>(a, s);
+  case 2: return launch_cfg<float, 128, 128, 4, 2, 3, 1>(a, s);
+  default: return launch_cfg<float, 128, 128, 4, 2, 4, 2>(a, s);
+  }
+}
+
+template <>
+int launch_simt_gemm<double>(const SimtGemmArgs<double> &a, cudaStream_t s) {
+  switch (simt_variant(true)) {
+  case 1: return launch_cfg<double, 128, 64, 4, 2, 4, 1>(a, s);
+  case 2: return launch_cfg<double, 128, 64, 4, 2, 4, 2>(a, s);
+  case 3: return launch_cfg<double, 64, 128, 2, 4, 4, 2>(a, s);
+  case 4: return launch_cfg<double, 128, 64, 2, 4, 4, 2>(a, s);
+  default: return launch_cfg<double, 128, 128, 4, 2, 3, 1>(a, s);  // fastest at n = 4096
+  }
 }
 
 template <typename T>
@@ -226,7 +252,5 @@ int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStrea
   return B200_OK;
 }
 
-template int launch_simt_gemm<float>(const SimtGemmArgs<float> &, cudaStream_t);
-template int launch_simt_gemm<double>(const SimtGemmArgs<double> &, cudaStream_t);
 template int launch_scale<float>(int, int, float, float *, long, long, int, cudaStream_t);
 template int launch_scale<double>(int, int, double, double *, long, long, int, cudaStream_t);

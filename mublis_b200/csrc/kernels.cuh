@@ -76,11 +76,11 @@ struct SimtConfig;
 
 template <>
 struct SimtConfig<float> {
-  static constexpr int BM = 128, BN = 128, BK = 16;
+  static constexpr int BM = 128, BN = 128, BK = 16;  // panel padding (tiles may be smaller)
 };
 template <>
 struct SimtConfig<double> {
-  static constexpr int BM = 128, BN = 64, BK = 16;
+  static constexpr int BM = 128, BN = 128, BK = 16;  // panel padding (tiles may be smaller)
 };
 
 template <typename T>

@@ -445,8 +445,13 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
 // The epilogue drains S_d from TMEM, adds ldexp(S_d, -7d) in FP64 into a
 // per-CTA tile workspace (L2-resident), and on the last phase writes
 // C = alpha * ldexp(W, e_i + f_j) + beta * C.  Phases (k-chunk, d) run from
-// the smallest d contribution to the largest; two TMEM accumulators let the
-// epilogue of one phase overlap the MMAs of the next.
+// the smallest d contribution to the largest.
+//
+// Tile: 256 x 256 per CTA, issued as two M=128 tcgen05 MMAs that share the
+// B tile, so every byte brought into shared memory feeds 1.5x the int8
+// products of a 128 x 256 tile (the int8 pipe outruns the L2 -> shared
+// memory feed otherwise).  The two accumulators fill all 512 TMEM columns;
+// the MMA issuer waits for the epilogue's drain at each phase boundary.
 
 namespace {
 
@@ -460,21 +465,23 @@ struct OzParams {
   double alpha, beta;
   double *c;
   long rs_c, cs_c;
-  double *work;  // gridDim.x tiles of 128 x 256 doubles
+  double *work;  // gridDim.x tiles of 256 x 256 doubles
   const unsigned long long *amax, *bmax;
   int *err;
 };
 
 struct OzCfg {
-  static constexpr int BM = 128, BN = 256, SWZ = 128, BK = 128, STAGES = 4;
+  static constexpr int BM = 256, BN = 256, SWZ = 128, BK = 128, STAGES = 3;
+  static constexpr int HALF_ROWS = 128;
   static constexpr int A_TILE = BM * SWZ, B_TILE = BN * SWZ;
   static constexpr int STAGE_BYTES = A_TILE + B_TILE;
   static constexpr int KSTEPS = SWZ / 32;
+  static constexpr int THREADS = 384, EPI_THREADS = 256;
   static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
   static constexpr uint32_t TMEM_COLS = 512;
 };
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(384, 1)
     tc_ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     OzParams p) {
   using C = OzCfg;
@@ -485,8 +492,8 @@ __global__ void __launch_bounds__(256, 1)
   uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE_BYTES);
   uint64_t *empty = full + STAGES;
   uint64_t *tfull = empty + STAGES;
-  uint64_t *tempty = tfull + 2;
-  uint64_t *drain = tempty + 2;
+  uint64_t *tempty = tfull + 1;
+  uint64_t *drain = tempty + 1;
   uint32_t *tmem_slot = (uint32_t *)(drain + 1);
   volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
@@ -496,10 +503,8 @@ __global__ void __launch_bounds__(256, 1)
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    for (int a = 0; a < 2; ++a) {
-      tc::mbar_init(&tfull[a], 1);
-      tc::mbar_init(&tempty[a], 128);
-    }
+    tc::mbar_init(tfull, 1);
+    tc::mbar_init(tempty, C::EPI_THREADS);
     tc::mbar_init(drain, 1);
     *abort_flag = 0;
     tc::fence_barrier_init();
@@ -554,8 +559,8 @@ __global__ void __launch_bounds__(256, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    constexpr uint32_t IDESC = tc::idesc_s8(C::BM, C::BN);
-    int stage = 0, acc = 0;
+    constexpr uint32_t IDESC = tc::idesc_s8(C::HALF_ROWS, C::BN);
+    int stage = 0;
     uint32_t phase = 0, acc_phase = 0;
     bool ok = true, any = false;
     for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
@@ -566,20 +571,22 @@ __global__ void __launch_bounds__(256, 1)
       for (int c0 = kb0; c0 < kb1 && ok; c0 += OZ_KCHUNK_BLOCKS) {
         const int c1 = min(kb1, c0 + OZ_KCHUNK_BLOCKS);
         for (int d = S + 1; d >= 2 && ok; --d) {
-          if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+          // The epilogue has drained the previous phase out of TMEM.
+          if (!tc::mbar_wait(tempty, acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
           tc::tc_fence_after();
-          const uint32_t dt = tmem_base + (uint32_t)(acc * C::BN);
           bool first = true;
           for (int t = max(1, d - S); t <= min(S, d - 1) && ok; ++t) {
             for (int kb = c0; kb < c1; ++kb) {
               if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
               tc::tc_fence_after();
-              const uint64_t ad = tc::smem_desc(sa(stage), C::SWZ);
+              const uint64_t a0 = tc::smem_desc(sa(stage), C::SWZ);
+              const uint64_t a1 = tc::smem_desc(sa(stage) + C::HALF_ROWS * C::SWZ, C::SWZ);
               const uint64_t bd = tc::smem_desc(sb(stage), C::SWZ);
 #pragma unroll
               for (int ks = 0; ks < C::KSTEPS; ++ks) {
-                tc::mma_i8(dt, ad + (uint64_t)((ks * 32) >> 4), bd + (uint64_t)((ks * 32) >> 4),
-                           IDESC, first ? 0u : 1u);
+                const uint64_t off = (uint64_t)((ks * 32) >> 4);
+                tc::mma_i8(tmem_base, a0 + off, bd + off, IDESC, first ? 0u : 1u);
+                tc::mma_i8(tmem_base + (uint32_t)C::BN, a1 + off, bd + off, IDESC, first ? 0u : 1u);
                 first = false;
               }
               tc::mma_commit(&empty[stage]);
@@ -588,8 +595,8 @@ __global__ void __launch_bounds__(256, 1)
             }
           }
           if (!ok) break;
-          tc::mma_commit(&tfull[acc]);
-          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+          tc::mma_commit(tfull);
+          acc_phase ^= 1;
         }
       }
     }
@@ -599,10 +606,13 @@ __global__ void __launch_bounds__(256, 1)
     }
   } else if (warp >= 4) {
     // ---------------- epilogue ----------------
-    const int ew = warp - 4;
-    const int row = ew * 32 + lane;
+    // Warps 4-7 drain the accumulator of rows 0-127, warps 8-11 the one of
+    // rows 128-255; each warp reads the TMEM lanes of its quadrant.
+    const int quad = warp & 3, half = (warp - 4) >> 2;
+    const int row = half * C::HALF_ROWS + quad * 32 + lane;  // tile row
+    const uint32_t lane_base =
+        tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * C::BN);
     double *W = p.work + (size_t)blockIdx.x * C::BM * C::BN;
-    int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
     for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
@@ -628,15 +638,14 @@ __global__ void __launch_bounds__(256, 1)
       int ph = 0;
       for (int cc = 0; cc < nchunks && ok; ++cc) {
         for (int d = S + 1; d >= 2; --d, ++ph) {
-          int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
+          int wok = tc::mbar_wait(tfull, acc_phase, abort_flag, p.err);
           if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
           tc::tc_fence_after();
           const bool last = ph == nph - 1;
 #pragma unroll 1
           for (int ch = 0; ch < C::BN / 16; ++ch) {
             uint32_t r[16];
-            tc::tmem_ld16(tmem_base + ((uint32_t)(ew * 32) << 16) +
-                              (uint32_t)(acc * C::BN + ch * 16), r);
+            tc::tmem_ld16(lane_base + (uint32_t)(ch * 16), r);
             tc::tmem_wait_ld();
             if (!row_ok) continue;
 #pragma unroll
@@ -658,8 +667,8 @@ __global__ void __launch_bounds__(256, 1)
             }
           }
           tc::tc_fence_before();
-          tc::mbar_arrive(&tempty[acc]);
-          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+          tc::mbar_arrive(tempty);
+          acc_phase ^= 1;
         }
       }
     }
@@ -764,7 +773,7 @@ int tc_run_ozaki(const b200_l3_desc_t *d) {
     }
     if (st == B200_OK) {
       B200ProfScope prof("tc_ozaki_i8", s);
-      tc_ozaki_kernel<<<grid, 256, C::SMEM, s>>>(ta, tb, p);
+      tc_ozaki_kernel<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);
       if (cudaGetLastError() != cudaSuccess) st = b200_set_error(B200_ECUDA, "ozaki launch failed");
     }
   }
