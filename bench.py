@@ -82,7 +82,7 @@ def kernel_flops(n: int) -> dict:
     the inverted diagonal blocks) on the direct kernel."""
     gemm_part = sum(flops(r, n) for r in ROUTINES if r != "trsm") + n * n * (n - 2 * DIRECT_K)
     direct = float(n * n * 2 * DIRECT_K)
-    return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part,
+    return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part, "dmma_dgemm": gemm_part,
             "direct_sgemm": direct, "direct_dgemm": direct}
 
 
@@ -290,8 +290,8 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
     """Precision forms at m = n = k = n (8192 by default; one call each,
     event-timed)."""
     out = {}
-    for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6"]),
-                         ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8"])):
+    for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6", "ozaki2"]),
+                         ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
         fill = getattr(lib, f"mublis_b200_fill_{p}")
         a, b, c = (torch.empty(n, n, dtype=dt, device="cuda") for _ in range(3))
         for i, x in enumerate((a, b, c)):
@@ -615,14 +615,22 @@ def main():
             avg_ms = total_ms / launches_k
             achieved = per_launch / (avg_ms * 1e-3) / 1e12
             is64 = dom.endswith("d") or "dgemm" in dom
+            tensor = dom.startswith("dmma")
             peak = FP64_NOMINAL_TFLOPS if is64 else FP32_NOMINAL_TFLOPS
             traffic = profile_traffic(dom)
-            roof = {"kernel": dom, "bound": "fp64_fma_pipe" if is64 else "fp32_fma_pipe",
+            if tensor:
+                bound = "tensor"
+                source = ("nominal FP64 tensor pipe (MEASURED_PEAKS.json has no FP64 figure): "
+                          "148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz; a register-only "
+                          "mma.sync m16n8k4 .f64 loop reaches 37.0 TF/s on this B200")
+            else:
+                bound = "fp64_fma_pipe" if is64 else "fp32_fma_pipe"
+                source = ("nominal (no FMA-pipe peak in MEASURED_PEAKS.json): 148 SMs x "
+                          + ("64 FP64" if is64 else "128 FP32") + " FMA lanes x 2 x 1965 MHz")
+            roof = {"kernel": dom, "bound": bound,
                     "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
                     "frac": round(achieved / peak, 4),
-                    "peak_source": "nominal (no FMA-pipe peak in MEASURED_PEAKS.json): 148 SMs x "
-                                   + ("64 FP64" if is64 else "128 FP32")
-                                   + " FMA lanes x 2 x 1965 MHz",
+                    "peak_source": source,
                     "traffic": traffic, "launches_per_step": launches_k / args.steps,
                     "share_of_step": round(total_ms / args.steps / ms, 4),
                     "bf16_tflops_measured": peaks.get("bf16_tflops"),

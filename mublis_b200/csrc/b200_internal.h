@@ -33,9 +33,17 @@ enum { B200_F32 = 0, B200_F64 = 1 };
  * BF16X3: FP32 operands split into bf16 hi+lo, three tcgen05 products per
  * k-block accumulated in FP32 (hi*hi + hi*lo + lo*hi).  BF16X6: three-term
  * split, six products.  OZAKI: FP64 via int8 slices with exact int32
- * accumulation (slice count in b200_form_t.slices). */
+ * accumulation (slice count in `slices`).  OZAKI2: FP64 via int8 residues
+ * modulo N coprime moduli, one exact int8 product per modulus and a CRT
+ * reconstruction (N in `slices`). */
 enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM_BF16X6 = 2,
-       B200_FORM_OZAKI = 3, B200_FORM_POLICY = 4 /* "auto": per-call size crossover */ };
+       B200_FORM_OZAKI = 3, B200_FORM_POLICY = 4 /* "auto": per-call size crossover */,
+       B200_FORM_OZAKI2 = 5 };
+
+/* Parse a form name ("plain", "bf16x3", "bf16x6", "ozaki[:s]", "ozaki2[:N]",
+ * "auto"); B200_FORM_AUTO for anything else.  *slices gets s or N when
+ * given (slices may be NULL). */
+int b200_parse_form(const char *s, int *slices);
 
 /* One product C(ji) := alpha * sum_t A_t B_t + beta * C over the domain of
  * `product`.  npairs is 1, or 2 for SYR2K (both pairs share the product's
@@ -85,7 +93,7 @@ int b200_set_error(int code, const char *where);
 const char *b200_last_error(void);
 int b200_get_default_form(int dtype);
 int b200_set_default_form(int dtype, int form, int slices);
-int b200_get_default_slices(void);
+int b200_get_default_slices(int dtype);
 
 /* Strided copies between caller host memory and a compact device buffer of
  * rows x cols with leading dimension ld (column-major).  The host side may

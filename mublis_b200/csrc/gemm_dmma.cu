@@ -1,0 +1,209 @@
+// gemm_dmma.cu -- plain FP64 GEMM on the FP64 tensor pipe: the device form
+// of the reference's five-loop driver (frame/l3/l3_driver.c:126-239) plus
+// its micro-kernel (include/mublis_instantiate.h:37-52) for double.
+//
+// B200 runs FP64 at the same peak on the tensor pipe (mma.sync .f64) as on
+// the FMA pipe (37 TF/s).  What the tensor path saves is operand traffic: a
+// warp's m16n8k4 MMA takes its 16x4 and 4x8 operands from registers the
+// warp loaded once, where an FMA-pipe kernel streams every operand through
+// shared memory per thread.  That traffic is what holds the FMA-pipe DGEMM
+// well below peak.
+//
+// Persistent CTAs (one per SM) walk the 128 x 128 output tiles.  Warp 8
+// produces: for every k-block of 16 it issues one 16 KB 1-D bulk copy (TMA)
+// per operand into a 4-stage shared-memory ring, completing on the stage's
+// mbarrier.  The panels are packed in fragment order (PACK_FRAG64), so a
+// k-block of a 128-row strip is contiguous and every warp's fragment load
+// is 512 contiguous bytes: no swizzle, no bank conflicts.  Warps 0-7
+// consume, each a 64 x 32 warp tile (4 x 4 m16n8k4 accumulators, 64 doubles
+// a thread), then release the stage to the producer.  Every wait is bounded
+// (tc_common.cuh); the producer waits for its own copies before it exits.
+//
+// Domain handling is the SIMT kernel's: ji skips tiles outside the written
+// triangle and masks partial tiles, jp/pi clip each tile's k-range, an empty
+// k-range writes beta * C, and beta == 0 never reads C.
+#include "kernels.cuh"
+#include "tc_common.cuh"
+
+namespace {
+
+constexpr int BM = B200_DMMA_TILE, BN = B200_DMMA_TILE, BK = B200_DMMA_BK, STAGES = 4;
+constexpr int CONSUMERS = 8;  // 2 (m) x 4 (n) warps of 64 x 32
+constexpr int THREADS = (CONSUMERS + 1) * 32;
+constexpr int TILE_BYTES = BM * BK * 8;  // 16 KB per operand per k-block
+constexpr int STAGE_BYTES = 2 * TILE_BYTES;
+constexpr int SMEM = STAGES * STAGE_BYTES + 128;
+constexpr int QUAD_DOUBLES = 8 * 32 * 2;  // one k-quad of a 128-row strip
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// Tile idx -> (tm, tn), rasterised in groups of 8 along M so that CTAs
+// running together share B strips in L2.
+__device__ __forceinline__ void tile_coords(const DmmaGemmArgs &p, int idx, int &tm, int &tn) {
+  constexpr int G = 8;
+  const int group = idx / (G * p.tiles_n);
+  const int first_m = group * G;
+  const int gsize = min(p.tiles_m - first_m, G);
+  const int in_group = idx % (G * p.tiles_n);
+  tm = first_m + in_group % gsize;
+  tn = in_group / gsize;
+}
+
+// false for a tile wholly outside the written triangle (l3_driver.c:145-147,
+// 165-171); else the tile's k-blocks [kt0, kt1) clipped to the product's
+// support (:130,148-150,163,171).
+__device__ __forceinline__ bool tile_krange(const DmmaGemmArgs &p, int tm, int tn, int &kt0,
+                                            int &kt1) {
+  const long m0 = (long)tm * BM, n0 = (long)tn * BN;
+  if (p.ji == MUBLIS_L3_LOWER && n0 >= m0 + BM) return false;
+  if (p.ji == MUBLIS_L3_UPPER && n0 + BN <= m0) return false;
+  long kb = 0, ke = p.k;
+  if (p.jp == MUBLIS_L3_LOWER) kb = max(kb, n0);       // j <= p
+  if (p.jp == MUBLIS_L3_UPPER) ke = min(ke, n0 + BN);  // j >= p
+  if (p.pi == MUBLIS_L3_LOWER) ke = min(ke, m0 + BM);  // p <= i
+  if (p.pi == MUBLIS_L3_UPPER) kb = max(kb, m0);       // p >= i
+  kt0 = (int)(kb / BK);
+  kt1 = ke > kb ? (int)((ke + BK - 1) / BK) : kt0;
+  return true;
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+    dmma_gemm_kernel(const __grid_constant__ DmmaGemmArgs p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  volatile int *abort_flag = (volatile int *)(empty + STAGES);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], CONSUMERS);
+    }
+    *abort_flag = 0;
+    tc::fence_barrier_init();
+  }
+  __syncthreads();
+  const int num_tiles = p.tiles_m * p.tiles_n;
+
+  if (warp == CONSUMERS) {
+    // ---------------- producer ----------------
+    if (lane != 0) return;
+    int stage = 0, issued = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+      int tm, tn, kt0, kt1;
+      tile_coords(p, idx, tm, tn);
+      if (!tile_krange(p, tm, tn, kt0, kt1)) continue;
+      const double *ga = p.ap + (long)tm * p.kq * 2 * 8 * 32;
+      const double *gb = p.bp + (long)tn * p.kq * 2 * 8 * 32;
+      for (int kt = kt0; kt < kt1; ++kt) {
+        if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+        unsigned char *dst = smem + stage * STAGE_BYTES;
+        tc::bulk_load_1d(dst, ga + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES, &full[stage]);
+        tc::bulk_load_1d(dst + TILE_BYTES, gb + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES,
+                         &full[stage]);
+        ++issued;
+        if (++stage == STAGES) { stage = 0; phase ^= 1; }
+      }
+    }
+    const int pending = issued < STAGES ? issued : STAGES;
+    for (int q = 0; q < pending; ++q) {
+      if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
+      if (!tc::mbar_wait_drain(&full[stage], phase)) break;
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  const int wm = warp & 1, wn = warp >> 1;
+  const int g = lane >> 2, t = lane & 3;
+  int stage = 0;
+  uint32_t phase = 0;
+  for (int idx = blockIdx.x; idx < num_tiles; idx += gridDim.x) {
+    int tm, tn, kt0, kt1;
+    tile_coords(p, idx, tm, tn);
+    if (!tile_krange(p, tm, tn, kt0, kt1)) continue;
+    double acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+    for (int kt = kt0; kt < kt1; ++kt) {
+      const int wok = tc::mbar_wait(&full[stage], phase, abort_flag, p.err);
+      if (!__all_sync(0xffffffffu, wok)) return;
+      const double2 *As = (const double2 *)(smem + stage * STAGE_BYTES) + wm * 4 * 32 + lane;
+      const double2 *Bs =
+          (const double2 *)(smem + stage * STAGE_BYTES + TILE_BYTES) + wn * 2 * 32 + lane;
+#pragma unroll
+      for (int ks = 0; ks < BK / 4; ++ks) {
+        double2 a[4], b[2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[(ks * 8 + i) * 32];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) b[j] = Bs[(ks * 8 + j) * 32];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            dmma(acc[i][j], a[i].x, a[i].y, (j & 1) ? b[j >> 1].y : b[j >> 1].x);
+      }
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&empty[stage]);
+      if (++stage == STAGES) { stage = 0; phase ^= 1; }
+    }
+
+    // Epilogue: accumulator e of block (i, j) is row g + 8 (e >> 1), column
+    // 2 t + (e & 1) of the 16 x 8 block.
+    const long m0 = (long)tm * BM + wm * 64, n0 = (long)tn * BN + wn * 32;
+    const double alpha = p.alpha, beta = p.beta;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long gi = m0 + i * 16 + g + 8 * h;
+        if (gi >= p.m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const long gj = n0 + j * 8 + 2 * t + e;
+            if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
+            double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+            double v = alpha * acc[i][j][2 * h + e];
+            if (beta != 0.0) v = fma(beta, *cij, v);
+            *cij = v;
+          }
+      }
+  }
+}
+
+}  // namespace
+
+int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s) {
+  const long tiles = (long)a.tiles_m * a.tiles_n;
+  if (tiles <= 0) return B200_OK;
+  if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "dgemm: too many tiles");
+  static bool configured = false;
+  if (!configured) {
+    B200_CUDA_TRY(
+        cudaFuncSetAttribute(dmma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    configured = true;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const int grid = (int)(tiles < sms ? tiles : sms);
+  B200ProfScope prof("dmma_dgemm", s);
+  dmma_gemm_kernel<<<grid, THREADS, SMEM, s>>>(a);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}

@@ -22,14 +22,44 @@ struct PackView {
 // view; anything past mn_len / k_len is zero.
 enum PackLayout {
   PACK_MN_MAJOR = 0,  // out[kk * ld + mn]       (SIMT kernels)
-  PACK_K_MAJOR = 1    // out[mn * ld + kk]       (tcgen05 kernels)
+  PACK_K_MAJOR = 1,   // out[mn * ld + kk]       (tcgen05 kernels)
+  PACK_FRAG64 = 2     // doubles in mma.m16n8k4 fragment order (FP64 MMA
+                      // kernel), ld = Kpad: see b200_frag64_offset
 };
 
+// Offset of element (mn, kk) of a PACK_FRAG64 panel (Kpad = ld, a multiple
+// of 16; Mpad a multiple of 128).  The panel is a sequence of 128-row
+// strips; a strip is a sequence of k-quads (4 consecutive kk); a k-quad of a
+// strip is 8 blocks of 16 rows, each 32 lanes x 2 doubles in the order an
+// mma.m16n8k4 .f64 fragment is held: lane = 4 (mn % 8) + kk % 4 holds rows
+// mn % 16 < 8 and >= 8 of its block as one 16-byte pair.  An A operand
+// strip is a 16-row block fragment (a0, a1) per lane; a B operand strip is
+// two 8-column fragments (b0 of columns 0-7, b0 of columns 8-15) per lane.
+// So one k-block of 16 of one strip is 16 KB contiguous, and every warp
+// fragment load is 512 contiguous bytes.
+__host__ __device__ inline long b200_frag64_offset(long mn, long kk, long kpad) {
+  return (((((mn >> 7) * (kpad >> 2) + (kk >> 2)) * 8 + ((mn & 127) >> 4)) * 32 +
+           (((mn & 7) << 2) | (kk & 3))) << 1) |
+         ((mn >> 3) & 1);
+}
+
 enum PackXform {
-  PACK_COPY = 0,        // T -> T
-  PACK_BF16_SPLIT = 1,  // f32 -> `terms` bf16 planes (hi, lo[, lo2])
-  PACK_INT8_SLICES = 2  // f64 -> `terms` int8 planes of 7-bit slices of
-                        // x * 2^(7 - e), e from the row/column abs-max
+  PACK_COPY = 0,         // T -> T
+  PACK_BF16_SPLIT = 1,   // f32 -> `terms` bf16 planes (hi, lo[, lo2])
+  PACK_INT8_SLICES = 2,  // f64 -> `terms` int8 planes of 7-bit slices of
+                         // x * 2^(7 - e), e from the row/column abs-max
+  PACK_INT8_MODULI = 3   // f64 -> `terms` int8 planes: the symmetric residues
+                         // of X = rint(x * 2^(bits - e)) modulo each modulus
+};
+
+// Pairwise coprime moduli (<= 256) of the modular (CRT) Ozaki form and the
+// constants that reduce an integer modulo each of them without division:
+// c16/c32/c48 = 2^16/2^32/2^48 mod m, magic = floor(2^32 / m) + 1.
+constexpr int B200_MAX_MODULI = 16;
+struct B200Moduli {
+  int n;
+  int m[B200_MAX_MODULI], c16[B200_MAX_MODULI], c32[B200_MAX_MODULI],
+      c48[B200_MAX_MODULI], magic[B200_MAX_MODULI];
 };
 
 struct PackOut {
@@ -37,12 +67,26 @@ struct PackOut {
   long ld;
   long plane_stride;  // elements between planes
   int layout, xform, terms;
-  const unsigned long long *absmax;  // PACK_INT8_SLICES: bits of max |x| per mn
+  const unsigned long long *absmax;  // INT8 forms: bits of max |x| per mn
+  int bits;                          // PACK_INT8_MODULI: |X| <= 2^bits
+  B200Moduli mod;                    // PACK_INT8_MODULI
 };
+
+// Symmetric residue of t modulo m in [-128, 127] (m <= 256, |t| < 2^26).
+// q = mulhi(t, floor(2^32/m) + 1) is floor(t/m) up to +-1 for |t| < 2^26,
+// so r = t - q m lies in [-m, 2m) and two conditional corrections bring it
+// to [0, m) before it is centred.
+__device__ __forceinline__ int b200_sym_mod(int t, int m, int magic) {
+  int r = t - __mulhi(t, magic) * m;
+  r += r < 0 ? m : 0;
+  r -= r >= m ? m : 0;
+  return r > 127 ? r - m : r;
+}
 
 // Bits of max |x| over kk for every mn of a logical operand view (the
 // Ozaki split's per-row / per-column scale), atomically max-merged into
 // absmax[mn] (which must start at 0).
+template <typename T>
 int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
                   unsigned long long *absmax, cudaStream_t s);
 
@@ -70,6 +114,21 @@ struct SimtGemmArgs {
   T alpha, beta;
   int jp, ji, pi;
 };
+
+// Plain FP64 GEMM on the FP64 tensor pipe over PACK_FRAG64 panels.
+struct DmmaGemmArgs {
+  const double *ap, *bp;  // PACK_FRAG64 panels, Mpad / Npad multiples of 128
+  long kq;                // Kpad / 4
+  double *c;
+  long rs_c, cs_c;
+  int m, n, k;
+  int tiles_m, tiles_n;
+  double alpha, beta;
+  int jp, ji, pi;
+  int *err;
+};
+int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s);
+constexpr int B200_DMMA_TILE = 128, B200_DMMA_BK = 16;
 
 template <typename T>
 struct SimtConfig;

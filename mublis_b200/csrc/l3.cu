@@ -8,9 +8,11 @@
 // triangle tiles through a temporary (:192-234).  Here each operand is packed
 // once for the whole call (one HBM pass, pack.cu) and the contraction kernel
 // tiles the entire output on the device.
+#include <cstdlib>
 #include <cstring>
 
 #include "kernels.cuh"
+#include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
 namespace {
@@ -53,8 +55,59 @@ int pack_pairs(const b200_l3_desc_t *d, const PackOut &oa, long mpad, const Pack
   return B200_OK;
 }
 
+// FP64 GEMM on the tensor pipe (gemm_dmma.cu) unless MUBLIS_B200_DGEMM=simt
+// selects the FMA-pipe kernel.
+bool use_dmma() {
+  static const bool on = [] {
+    const char *e = getenv("MUBLIS_B200_DGEMM");
+    return !(e && !strcmp(e, "simt"));
+  }();
+  return on;
+}
+
+int run_dmma(const b200_l3_desc_t *d) {
+  cudaStream_t s = b200_cur_stream();
+  const long ktot = (long)d->k * d->npairs;
+  const long mpad = b200_round_up(d->m, B200_DMMA_TILE);
+  const long npad = b200_round_up(d->n, B200_DMMA_TILE);
+  const long kpad = b200_round_up(ktot, B200_DMMA_BK);
+  void *ap = nullptr, *bp = nullptr;
+  B200_TRY(b200_alloc(&ap, sizeof(double) * mpad * kpad));
+  int st = b200_alloc(&bp, sizeof(double) * npad * kpad);
+  if (st == B200_OK) {
+    PackOut oa{ap, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
+    PackOut ob{bp, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
+    st = pack_pairs<double>(d, oa, mpad, ob, npad, kpad, s);
+  }
+  if (st == B200_OK) {
+    DmmaGemmArgs g;
+    g.ap = (const double *)ap;
+    g.bp = (const double *)bp;
+    g.kq = kpad / 4;
+    g.c = (double *)d->c;
+    g.rs_c = d->rs_c;
+    g.cs_c = d->cs_c;
+    g.m = d->m;
+    g.n = d->n;
+    g.k = (int)ktot;
+    g.tiles_m = (int)(mpad / B200_DMMA_TILE);
+    g.tiles_n = (int)(npad / B200_DMMA_TILE);
+    g.alpha = d->alpha;
+    g.beta = d->beta;
+    g.jp = d->product.domain.jp;
+    g.ji = d->product.domain.ji;
+    g.pi = d->product.domain.pi;
+    g.err = b200_device_error_word();
+    st = launch_dmma_gemm(g, s);
+  }
+  b200_free(ap);
+  b200_free(bp);
+  return st;
+}
+
 template <typename T>
 int run_plain(const b200_l3_desc_t *d) {
+  if (sizeof(T) == 8 && use_dmma()) return run_dmma(d);
   using C = SimtConfig<T>;
   cudaStream_t s = b200_cur_stream();
   const long ktot = (long)d->k * d->npairs;
@@ -111,14 +164,13 @@ extern "C" int b200_l3_run(const b200_l3_desc_t *d) {
                               d->product.domain.ji);
   const int form = resolve_form(d);
   if (form == B200_FORM_BF16X3 || form == B200_FORM_BF16X6) return tc_run_bf16(d, form);
-  if (form == B200_FORM_OZAKI) {
+  if (form == B200_FORM_OZAKI || form == B200_FORM_OZAKI2) {
+    b200_l3_desc_t e = *d;
+    e.form = form;
     if (d->form == B200_FORM_POLICY || (d->form == B200_FORM_AUTO &&
-                                        b200_get_default_form(d->dtype) == B200_FORM_POLICY)) {
-      b200_l3_desc_t e = *d;
-      e.slices = 8;
-      return tc_run_ozaki(&e);
-    }
-    return tc_run_ozaki(d);
+                                        b200_get_default_form(d->dtype) == B200_FORM_POLICY))
+      e.slices = form == B200_FORM_OZAKI ? 8 : 0;  // 0: the form's default count
+    return tc_run_ozaki(&e);
   }
   if (d->dtype == B200_F32) return run_plain<float>(d);
   return run_plain<double>(d);

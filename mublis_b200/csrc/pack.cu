@@ -63,6 +63,24 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
   }
   __syncthreads();
 
+  if (o.layout == PACK_FRAG64) {
+    // Fragment-order panel (doubles only): each thread stores the pair
+    // (mn, mn + 8) of one kk as 16 bytes; a warp covers one 16-row block of
+    // one k-quad (512 contiguous bytes when kk_base is a multiple of 4).
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int combo = ty + 8 * q;  // 2 blocks of 16 rows x 8 k-quads
+        const int mn_l = (combo & 1) * 16 + (tx >> 2), kk_l = (combo >> 1) * 4 + (tx & 3);
+        const long mn = mn_base + mn_l, kk = kk_base + kk_l;
+        if (kk >= kk1) continue;
+        *reinterpret_cast<double2 *>((double *)o.out + b200_frag64_offset(mn, kk, o.ld)) =
+            make_double2(tile[kk_l][mn_l], tile[kk_l][mn_l + 8]);
+      }
+    }
+    return;
+  }
+
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     int a = tx, b = ty + 8 * q;
@@ -83,6 +101,23 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
         double q = trunc(r);
         out[off + t * o.plane_stride] = (int8_t)(int)q;
         r = (r - q) * 128.0;
+      }
+    } else if (o.xform == PACK_INT8_MODULI) {
+      // X = rint(x * 2^(bits - e)) is an integer with |X| <= 2^bits <= 2^56,
+      // exact in FP64.  Cut it into 16-bit pieces X = hh 2^48 + hl 2^32 +
+      // lh 2^16 + ll (every step exact), so that X mod m is the residue of
+      // hh c48 + hl c32 + lh c16 + ll, an int32 below 2^26 in magnitude.
+      int8_t *out = (int8_t *)o.out;
+      const double x = rint(ldexp((double)val, o.bits - b200_scale_exp(o.absmax[mn])));
+      const double hh = floor(x * 0x1p-48), x1 = fma(-hh, 0x1p48, x);
+      const double hl = floor(x1 * 0x1p-32), x2 = fma(-hl, 0x1p32, x1);
+      const double lh = floor(x2 * 0x1p-16), ll = fma(-lh, 0x1p16, x2);
+      const int ihh = (int)hh, ihl = (int)hl, ilh = (int)lh, ill = (int)ll;
+#pragma unroll
+      for (int t = 0; t < B200_MAX_MODULI; ++t) {  // constant indices: no local copy
+        if (t >= o.terms) break;
+        const int v = ihh * o.mod.c48[t] + ihl * o.mod.c32[t] + ilh * o.mod.c16[t] + ill;
+        out[off + t * o.plane_stride] = (int8_t)b200_sym_mod(v, o.mod.m[t], o.mod.magic[t]);
       }
     } else {
       __nv_bfloat16 *out = (__nv_bfloat16 *)o.out;
@@ -132,6 +167,7 @@ __global__ void __launch_bounds__(256) absmax_kernel(PackView v, bool b_side, lo
 
 }  // namespace
 
+template <typename T>
 int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
                   unsigned long long *absmax, cudaStream_t s) {
   if (mn_len <= 0 || k_len <= 0) return B200_OK;
@@ -141,7 +177,7 @@ int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
   dim3 grid((unsigned)b200_ceil_div(mn_len, 32), (unsigned)b200_ceil_div(k_len, 32));
   if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
   B200ProfScope prof("absmax", s);
-  absmax_kernel<double><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, mn_fast, absmax);
+  absmax_kernel<T><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, mn_fast, absmax);
   B200_LAUNCH_CHECK();
   return B200_OK;
 }
@@ -165,3 +201,7 @@ template int launch_pack<float>(const PackView &, bool, long, long, long, long, 
                                 const PackOut &, cudaStream_t);
 template int launch_pack<double>(const PackView &, bool, long, long, long, long, long,
                                  const PackOut &, cudaStream_t);
+template int launch_absmax<float>(const PackView &, bool, long, long, unsigned long long *,
+                                  cudaStream_t);
+template int launch_absmax<double>(const PackView &, bool, long, long, unsigned long long *,
+                                   cudaStream_t);

@@ -27,7 +27,7 @@ int g_device = 0;
 std::atomic<unsigned long long> g_launches{0};
 
 int g_default_form[2] = {B200_FORM_PLAIN, B200_FORM_PLAIN};
-int g_default_slices = 0;
+int g_default_slices[2] = {0, 0};  // per dtype: slice / modulus count, 0 = form default
 
 thread_local cudaStream_t t_stream = nullptr;
 thread_local bool t_stream_owned = false;
@@ -40,19 +40,6 @@ struct ProfRec {
 std::mutex g_prof_mu;
 std::vector<ProfRec> g_prof;
 std::atomic<int> g_prof_on{0};
-
-int parse_form(const char *s, int *slices) {
-  if (!s || !*s) return B200_FORM_AUTO;
-  if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
-  if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
-  if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
-  if (!strcmp(s, "auto")) return B200_FORM_POLICY;
-  if (!strncmp(s, "ozaki", 5)) {
-    if (s[5] == ':' && slices) *slices = atoi(s + 6);
-    return B200_FORM_OZAKI;
-  }
-  return B200_FORM_AUTO;
-}
 
 void do_init() {
   int count = 0;
@@ -78,14 +65,17 @@ void do_init() {
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
   }
   int slices = 0;
-  int sf = parse_form(getenv("MUBLIS_B200_SFORM"), nullptr);
-  int df = parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
+  int sslices = 0;
+  int sf = b200_parse_form(getenv("MUBLIS_B200_SFORM"), &sslices);
+  int df = b200_parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
   if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6 ||
-      sf == B200_FORM_POLICY)
+      sf == B200_FORM_OZAKI2 || sf == B200_FORM_POLICY)
     g_default_form[B200_F32] = sf;
-  if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI || df == B200_FORM_POLICY)
+  if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI || df == B200_FORM_OZAKI2 ||
+      df == B200_FORM_POLICY)
     g_default_form[B200_F64] = df;
-  if (slices > 0) g_default_slices = slices;
+  if (slices > 0) g_default_slices[B200_F64] = slices;
+  if (sslices > 0) g_default_slices[B200_F32] = sslices;
   g_init_status = B200_OK;
 }
 
@@ -180,18 +170,38 @@ int b200_set_error(int code, const char *where) {
 
 const char *b200_last_error(void) { return t_error; }
 
+int b200_parse_form(const char *s, int *slices) {
+  if (!s || !*s) return B200_FORM_AUTO;
+  if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
+  if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
+  if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
+  if (!strcmp(s, "auto")) return B200_FORM_POLICY;
+  const bool mod = !strncmp(s, "ozaki2", 6);
+  if (mod || !strncmp(s, "ozaki", 5)) {
+    const char *tail = s + (mod ? 6 : 5);
+    if (*tail == ':') {
+      if (slices) *slices = atoi(tail + 1);
+    } else if (*tail) {
+      return B200_FORM_AUTO;
+    }
+    return mod ? B200_FORM_OZAKI2 : B200_FORM_OZAKI;
+  }
+  return B200_FORM_AUTO;
+}
+
 int b200_get_default_form(int dtype) { return g_default_form[dtype == B200_F64]; }
-int b200_get_default_slices(void) { return g_default_slices; }
+int b200_get_default_slices(int dtype) { return g_default_slices[dtype == B200_F64]; }
 
 int b200_set_default_form(int dtype, int form, int slices) {
   if (dtype == B200_F32 && form != B200_FORM_PLAIN && form != B200_FORM_BF16X3 &&
-      form != B200_FORM_BF16X6 && form != B200_FORM_POLICY)
+      form != B200_FORM_BF16X6 && form != B200_FORM_OZAKI2 && form != B200_FORM_POLICY)
     return B200_EINVAL;
   if (dtype == B200_F64 && form != B200_FORM_PLAIN && form != B200_FORM_OZAKI &&
-      form != B200_FORM_POLICY)
+      form != B200_FORM_OZAKI2 && form != B200_FORM_POLICY)
     return B200_EINVAL;
   g_default_form[dtype == B200_F64] = form;
-  if (slices > 0) g_default_slices = slices;
+  // The count belongs to the form just set (0: that form's own default).
+  g_default_slices[dtype == B200_F64] = slices > 0 ? slices : 0;
   return B200_OK;
 }
 
@@ -266,7 +276,7 @@ void *mublis_b200_get_stream(void) {
 int mublis_b200_set_form(char dtype, const char *form) {
   B200_TRY(b200_init());
   int slices = 0;
-  int f = parse_form(form, &slices);
+  int f = b200_parse_form(form, &slices);
   if (f == B200_FORM_AUTO) return B200_EINVAL;
   return b200_set_default_form(dtype == 'd' ? B200_F64 : B200_F32, f, slices);
 }

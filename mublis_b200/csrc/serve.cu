@@ -124,7 +124,8 @@ size_t scratch_estimate(const Req &r) {
   if (f == B200_FORM_POLICY) f = r.dtype == B200_F64 ? B200_FORM_OZAKI : B200_FORM_BF16X6;
   if (f == B200_FORM_BF16X6) return 3 * (mp + np) * kp * 2;
   if (f == B200_FORM_BF16X3) return 2 * (mp + np) * kp * 2;
-  if (f == B200_FORM_OZAKI) return 12 * (mp + np) * kp + 148 * 128 * 256 * 8;
+  if (f == B200_FORM_OZAKI) return 12 * (mp + np) * kp + 148 * 256 * 256 * 8;
+  if (f == B200_FORM_OZAKI2) return 16 * (mp + np) * kp + 148 * 16 * 256 * 256;
   return (mp + np) * kp * elt;
 }
 
@@ -277,19 +278,6 @@ int submit_and_wait(mublis_b200_server *S, Req &r) {
   return B200_OK;
 }
 
-int parse_form(const char *s, int *slices) {
-  if (!s || !*s) return B200_FORM_AUTO;
-  if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
-  if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
-  if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
-  if (!strcmp(s, "auto")) return B200_FORM_POLICY;
-  if (!strncmp(s, "ozaki", 5)) {
-    if (s[5] == ':') *slices = atoi(s + 6);
-    return B200_FORM_OZAKI;
-  }
-  return B200_FORM_AUTO;
-}
-
 double l3_flops(const b200_l3_desc_t &d) {
   double m = d.m, n = d.n, k = (double)d.k * d.npairs;
   if (d.product.domain.ji != MUBLIS_L3_ALL) return m * (m + 1) * k;  // SYRK / SYR2K
@@ -312,7 +300,7 @@ extern "C" int b200_serve_l3(const b200_l3_desc_t *d) {
   r.small = b200_l3_is_plain_gemm(d) && mx <= S->cfg.small_max_dim;
   if (!r.small && r.l3.form == B200_FORM_AUTO) {
     int slices = 0;
-    int f = parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
+    int f = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
     r.l3.form = f;
     if (slices) r.l3.slices = slices;
   }
@@ -331,7 +319,7 @@ extern "C" int b200_serve_trsm(const b200_trsm_desc_t *d) {
   r.small = d->m <= 256 && d->alpha != 0.0;
   if (!r.small && r.tr.form == B200_FORM_AUTO) {
     int slices = 0;
-    r.tr.form = parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
+    r.tr.form = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
     if (slices) r.tr.slices = slices;
   }
   r.scratch = r.small ? 0 : scratch_estimate(r);

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(384, 1)
     int pending = issued < STAGES ? issued : STAGES;
     for (int q = 0; q < pending; ++q) {
       if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
-      if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) break;
+      if (!tc::mbar_wait_drain(&full[stage], phase)) break;
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
@@ -435,17 +435,40 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
 
 // ---- Ozaki split-integer FP64 ---------------------------------------------------
 //
-// op(A) row i is scaled by 2^-e_i and op(B) column j by 2^-f_j (e, f from the
-// abs-max, so scaled values lie in (-1, 1)), and each scaled value is cut
-// into s signed 7-bit slices: a = 2^e_i sum_t A_t 2^-7t, b = 2^f_j sum_u B_u
-// 2^-7u (pack.cu).  Then C = 2^(e_i + f_j) sum_d 2^-7d S_d with
-// S_d = sum_{t+u=d} A_t B_u, keeping the diagonals d <= s + 1.  Every S_d is
-// an exact int32 tcgen05 (kind::i8) accumulation as long as
-// s * kchunk * 127^2 < 2^31, so k is processed in chunks of 8192 and s <= 12.
-// The epilogue drains S_d from TMEM, adds ldexp(S_d, -7d) in FP64 into a
-// per-CTA tile workspace (L2-resident), and on the last phase writes
-// C = alpha * ldexp(W, e_i + f_j) + beta * C.  Phases (k-chunk, d) run from
-// the smallest d contribution to the largest.
+// Two forms share one persistent kernel (template MOD).
+//
+// Slices (MOD = false; Ozaki, Ogita, Oishi, Rump 2012, with the integer-MMA
+// formulation of Mukunoki et al. and Uchino et al.).  op(A) row i is scaled
+// by 2^-e_i and op(B) column j by 2^-f_j (e, f from the abs-max, so scaled
+// values lie in (-1, 1)), and each scaled value is cut into s signed 7-bit
+// slices: a = 2^e_i sum_t A_t 2^-7t, b = 2^f_j sum_u B_u 2^-7u (pack.cu).
+// Then C = 2^(e_i + f_j) sum_d 2^-7d S_d with S_d = sum_{t+u=d} A_t B_u,
+// keeping the diagonals d <= s + 1.  Every S_d is an exact int32 tcgen05
+// (kind::i8) accumulation as long as s * kchunk * 127^2 < 2^31, so k is
+// processed in chunks of 8192 and s <= 12.  The epilogue drains S_d from
+// TMEM, adds ldexp(S_d, -7d) in FP64 into a per-CTA tile workspace
+// (L2-resident), and on the last phase writes C = alpha * ldexp(W, e_i +
+// f_j) + beta * C.  Phases (k-chunk, d) run from the smallest d
+// contribution to the largest.
+//
+// Moduli (MOD = true; Ozaki scheme II, Ozaki, Uchino and Imamura 2025).
+// op(A) row i becomes the integer row A'_i = rint(a_i * 2^(pa - e_i)) and
+// op(B) column j becomes B'_j = rint(b_j * 2^(pb - f_j)), so |A'|, |B'| are
+// at most 2^pa, 2^pb.  For N pairwise coprime moduli m_l <= 256 with
+// product M, pa + pb is chosen so that k 2^(pa+pb) < M/2 (1 - 2^-30): the
+// integer product C' = A'B' is then fixed by its residues modulo every m_l.
+// Each residue plane A'_l = A' mod m_l (int8, symmetric) is packed once, and
+// one int8 GEMM per modulus gives C'_l = A'_l B'_l exactly in int32 (k in
+// chunks of 65536 keeps |C'_l| < 2^30).  The epilogue reduces C'_l mod m_l
+// into a byte per element of a per-CTA residue workspace; after the tile's
+// last modulus it reconstructs C' by the Chinese remainder theorem,
+// C' = sum_l r_l W_l - q M with W_l = (M/m_l) ((M/m_l)^-1 mod m_l) and
+// q = round(sum / M), and writes C = alpha 2^(e_i + f_j - pa - pb) C' +
+// beta C.  The CRT sum is exact in FP64: W_l and M are cut at bits 42 and 84
+// into three 42-bit levels, each level's sum of N products r_l W_l,lev
+// stays below 2^53 units of that level, and the top level minus q M_0 is
+// exact as well.  N int8 GEMMs (16 give ~55-bit inputs) replace the
+// s(s+1)/2 of the slice form.
 //
 // Tile: 256 x 256 per CTA, issued as two M=128 tcgen05 MMAs that share the
 // B tile, so every byte brought into shared memory feeds 1.5x the int8
@@ -456,18 +479,30 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
 namespace {
 
 constexpr int OZ_MAX_SLICES = 12;
-constexpr int OZ_KCHUNK_BLOCKS = 64;  // 64 x 128 = 8192 k per exact int32 chunk
+constexpr int OZ_KCHUNK_BLOCKS = 64;    // 64 x 128 = 8192 k per exact int32 chunk
+constexpr int OZ2_KCHUNK_BLOCKS = 512;  // 512 x 128 = 65536 k (|C'_l| < 2^30)
+
+// CRT reconstruction constants of the modular form (host-computed).
+struct OzCrt {
+  double w[B200_MAX_MODULI][3];  // W_l cut into 42-bit levels at bits 84 / 42 / 0
+  double mlev[3];                // M cut the same way
+  double inv_m;                  // 1 / M
+  int m[B200_MAX_MODULI], c16[B200_MAX_MODULI], magic[B200_MAX_MODULI];
+  int bits;                      // pa + pb
+};
 
 struct OzParams {
   TileWalk w;
   long mpad, npad;
-  int slices;
+  int slices;  // slice count, or modulus count N of the modular form
   double alpha, beta;
-  double *c;
+  void *c;  // double (both forms) or float (modular form)
   long rs_c, cs_c;
-  double *work;  // gridDim.x tiles of 256 x 256 doubles
+  void *work;  // slices: gridDim.x tiles of 256 x 256 doubles;
+               // moduli: gridDim.x x N x 256 x 256 residue bytes
   const unsigned long long *amax, *bmax;
   int *err;
+  OzCrt crt;
 };
 
 struct OzCfg {
@@ -481,11 +516,41 @@ struct OzCfg {
   static constexpr uint32_t TMEM_COLS = 512;
 };
 
+// Phases of one k-chunk and the (t, u) plane pairs of each phase.  Slices:
+// phase ph is diagonal d = s + 1 - ph with t = max(1, d - s) .. min(s, d - 1),
+// u = d - t.  Moduli: phase l is the single pair (l + 1, l + 1).
+template <bool MOD>
+__device__ __forceinline__ void oz_pairs(int S, int ph, int &t0, int &t1, int &d) {
+  if (MOD) {
+    t0 = t1 = ph + 1;
+    d = 2 * (ph + 1);
+  } else {
+    d = S + 1 - ph;
+    t0 = max(1, d - S);
+    t1 = min(S, d - 1);
+  }
+}
+
+// CRT of one element from its N residues (the modular form's last step).
+__device__ __forceinline__ double oz_crt(const OzCrt &k, double s0, double s1, double s2) {
+  // All three levels enter q: with few moduli (M below 2^84) the low levels
+  // carry most of the sum.  |S/M| < 2^11 and the argument's error is below
+  // 2^-40, while the pa + pb margin keeps S/M at least 2^-21 away from a
+  // half-integer, so q is exact.
+  const double q = rint(fma(s0, k.inv_m, fma(s1, k.inv_m, s2 * k.inv_m)));
+  const double t0 = fma(-q, k.mlev[0], s0);  // exact: |t0| < 2^126, a multiple of 2^84
+  const double t1 = fma(-q, k.mlev[1], s1);
+  const double t2 = fma(-q, k.mlev[2], s2);
+  return (t0 + t1) + t2;
+}
+
+template <bool MOD, typename TC>
 __global__ void __launch_bounds__(384, 1)
     tc_ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    OzParams p) {
+                    const __grid_constant__ OzParams p) {
   using C = OzCfg;
   constexpr int STAGES = C::STAGES;
+  constexpr int KCHUNK = MOD ? OZ2_KCHUNK_BLOCKS : OZ_KCHUNK_BLOCKS;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem =
       (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -533,10 +598,12 @@ __global__ void __launch_bounds__(384, 1)
       w.coords(idx, tm, tn);
       if (!w.valid(tm, tn)) continue;
       w.krange(tm, tn, kb0, kb1);
-      for (int c0 = kb0; c0 < kb1 && ok; c0 += OZ_KCHUNK_BLOCKS) {
-        const int c1 = min(kb1, c0 + OZ_KCHUNK_BLOCKS);
-        for (int d = S + 1; d >= 2 && ok; --d) {
-          for (int t = max(1, d - S); t <= min(S, d - 1) && ok; ++t) {
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += KCHUNK) {
+        const int c1 = min(kb1, c0 + KCHUNK);
+        for (int ph = 0; ph < S && ok; ++ph) {
+          int t0, t1, d;
+          oz_pairs<MOD>(S, ph, t0, t1, d);
+          for (int t = t0; t <= t1 && ok; ++t) {
             const int u = d - t;
             for (int kb = c0; kb < c1; ++kb) {
               if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
@@ -555,7 +622,7 @@ __global__ void __launch_bounds__(384, 1)
     int pending = issued < STAGES ? issued : STAGES;
     for (int q = 0; q < pending; ++q) {
       if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
-      if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) break;
+      if (!tc::mbar_wait_drain(&full[stage], phase)) break;
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
@@ -568,14 +635,16 @@ __global__ void __launch_bounds__(384, 1)
       w.coords(idx, tm, tn);
       if (!w.valid(tm, tn)) continue;
       w.krange(tm, tn, kb0, kb1);
-      for (int c0 = kb0; c0 < kb1 && ok; c0 += OZ_KCHUNK_BLOCKS) {
-        const int c1 = min(kb1, c0 + OZ_KCHUNK_BLOCKS);
-        for (int d = S + 1; d >= 2 && ok; --d) {
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += KCHUNK) {
+        const int c1 = min(kb1, c0 + KCHUNK);
+        for (int ph = 0; ph < S && ok; ++ph) {
+          int t0, t1, d;
+          oz_pairs<MOD>(S, ph, t0, t1, d);
           // The epilogue has drained the previous phase out of TMEM.
           if (!tc::mbar_wait(tempty, acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
           tc::tc_fence_after();
           bool first = true;
-          for (int t = max(1, d - S); t <= min(S, d - 1) && ok; ++t) {
+          for (int t = t0; t <= t1 && ok; ++t) {
             for (int kb = c0; kb < c1; ++kb) {
               if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
               tc::tc_fence_after();
@@ -612,7 +681,10 @@ __global__ void __launch_bounds__(384, 1)
     const int row = half * C::HALF_ROWS + quad * 32 + lane;  // tile row
     const uint32_t lane_base =
         tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * C::BN);
-    double *W = p.work + (size_t)blockIdx.x * C::BM * C::BN;
+    double *W = (double *)p.work + (size_t)blockIdx.x * C::BM * C::BN;
+    // Residue workspace of the modular form: [l][16-column chunk][row][16 B],
+    // so a warp's 16-byte stores and loads are 512 contiguous bytes.
+    unsigned char *R = (unsigned char *)p.work + (size_t)blockIdx.x * S * C::BM * C::BN;
     uint32_t acc_phase = 0;
     bool ok = true;
     for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
@@ -628,47 +700,108 @@ __global__ void __launch_bounds__(384, 1)
           for (int j = 0; j < C::BN; ++j) {
             const long gj = (long)tn * C::BN + j;
             if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
-            double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
-            *cij = p.beta != 0.0 ? p.beta * *cij : 0.0;
+            TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
+            *cij = p.beta != 0.0 ? (TC)(p.beta * (double)*cij) : TC(0);
           }
         continue;
       }
-      const int nchunks = (kb1 - kb0 + OZ_KCHUNK_BLOCKS - 1) / OZ_KCHUNK_BLOCKS;
+      const int nchunks = (kb1 - kb0 + KCHUNK - 1) / KCHUNK;
       const int nph = nchunks * S;
       int ph = 0;
       for (int cc = 0; cc < nchunks && ok; ++cc) {
-        for (int d = S + 1; d >= 2; --d, ++ph) {
+        for (int pl = 0; pl < S; ++pl, ++ph) {
           int wok = tc::mbar_wait(tfull, acc_phase, abort_flag, p.err);
           if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
           tc::tc_fence_after();
           const bool last = ph == nph - 1;
+          if constexpr (MOD) {
+            const int m = p.crt.m[pl], c16 = p.crt.c16[pl], magic = p.crt.magic[pl];
+            uint4 *Rl = (uint4 *)(R + (size_t)pl * C::BM * C::BN) + row;
 #pragma unroll 1
-          for (int ch = 0; ch < C::BN / 16; ++ch) {
-            uint32_t r[16];
-            tc::tmem_ld16(lane_base + (uint32_t)(ch * 16), r);
-            tc::tmem_wait_ld();
-            if (!row_ok) continue;
+            for (int ch = 0; ch < C::BN / 16; ++ch) {
+              uint32_t r[16];
+              tc::tmem_ld16(lane_base + (uint32_t)(ch * 16), r);
+              tc::tmem_wait_ld();
+              uint4 prev = cc > 0 ? Rl[ch * C::BM] : make_uint4(0, 0, 0, 0);
+              uint32_t out[4] = {0, 0, 0, 0};
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int col = ch * 16 + j;
-              double *wp = W + row + (size_t)col * C::BM;
-              double v = ldexp((double)(int)r[j], -7 * d);
-              if (ph > 0) v += *wp;
-              if (!last) {
-                *wp = v;
-                continue;
+              for (int j = 0; j < 16; ++j) {
+                const int v = (int)r[j];  // |v| < 2^30
+                int res = b200_sym_mod((v >> 16) * c16 + (v & 0xffff), m, magic);
+                if (cc > 0) {
+                  const uint32_t word = j < 4 ? prev.x : j < 8 ? prev.y : j < 12 ? prev.z : prev.w;
+                  const int pr = (int)(int8_t)(word >> (8 * (j & 3)));
+                  res = b200_sym_mod(res + pr, m, magic);
+                }
+                out[j >> 2] |= (uint32_t)(res & 0xff) << (8 * (j & 3));
               }
-              const long gj = (long)tn * C::BN + col;
-              if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
-              double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
-              double out = p.alpha * ldexp(v, ei + b200_scale_exp(p.bmax[gj]));
-              if (p.beta != 0.0) out = fma(p.beta, *cij, out);
-              *cij = out;
+              Rl[ch * C::BM] = make_uint4(out[0], out[1], out[2], out[3]);
+            }
+          } else {
+#pragma unroll 1
+            for (int ch = 0; ch < C::BN / 16; ++ch) {
+              uint32_t r[16];
+              tc::tmem_ld16(lane_base + (uint32_t)(ch * 16), r);
+              tc::tmem_wait_ld();
+              if (!row_ok) continue;
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                const int col = ch * 16 + j;
+                double *wp = W + row + (size_t)col * C::BM;
+                double v = ldexp((double)(int)r[j], -7 * (S + 1 - pl));
+                if (ph > 0) v += *wp;
+                if (!last) {
+                  *wp = v;
+                  continue;
+                }
+                const long gj = (long)tn * C::BN + col;
+                if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+                TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
+                double out = p.alpha * ldexp(v, ei + b200_scale_exp(p.bmax[gj]));
+                if (p.beta != 0.0) out = fma(p.beta, (double)*cij, out);
+                *cij = (TC)out;
+              }
             }
           }
           tc::tc_fence_before();
           tc::mbar_arrive(tempty);
           acc_phase ^= 1;
+        }
+      }
+      if constexpr (MOD) {
+        // TMEM is released; reconstruct C' from this thread's own residues
+        // while the MMAs of the next tile run.
+        if (!ok || !row_ok) continue;
+        const OzCrt &k = p.crt;
+        const int sh = ei - k.bits;
+#pragma unroll 1
+        for (int ch8 = 0; ch8 < C::BN / 8; ++ch8) {
+          double s0[8], s1[8], s2[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) s0[j] = s1[j] = s2[j] = 0.0;
+          const uint2 *base = (const uint2 *)((const uint4 *)R + (size_t)(ch8 >> 1) * C::BM + row) +
+                              (ch8 & 1);
+#pragma unroll 1
+          for (int l = 0; l < S; ++l) {
+            const uint2 v = base[(size_t)l * (C::BM * C::BN / 8)];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const double rr = (double)(int8_t)((j < 4 ? v.x : v.y) >> (8 * (j & 3)));
+              s0[j] = fma(rr, k.w[l][0], s0[j]);
+              s1[j] = fma(rr, k.w[l][1], s1[j]);
+              s2[j] = fma(rr, k.w[l][2], s2[j]);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const long gj = (long)tn * C::BN + ch8 * 8 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
+            const double cp = oz_crt(k, s0[j], s1[j], s2[j]);
+            double out = p.alpha * ldexp(cp, sh + b200_scale_exp(p.bmax[gj]));
+            if (p.beta != 0.0) out = fma(p.beta, (double)*cij, out);
+            *cij = (TC)out;
+          }
         }
       }
     }
@@ -682,21 +815,81 @@ __global__ void __launch_bounds__(384, 1)
   }
 }
 
+// The modular form's moduli: the largest pairwise coprime integers <= 256.
+constexpr int OZ2_MODULI[B200_MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                             229, 227, 223, 217, 211, 199, 197, 193};
+
+// Host set-up of the modular form for N moduli and inner dimension k: the
+// residue constants for packing and the epilogue, the CRT levels, and the
+// scale exponents pa (rows of op(A)) and pb (columns of op(B)), each at most
+// pmax (bits beyond the input's significand buy nothing).
+int oz2_setup(int N, long k, int pmax, B200Moduli *mod, OzCrt *crt, int *pa, int *pb) {
+  typedef unsigned __int128 u128;
+  u128 M = 1;
+  for (int l = 0; l < N; ++l) M *= (u128)OZ2_MODULI[l];
+  long double log2m = 0.0L;
+  for (int l = 0; l < N; ++l) log2m += log2l((long double)OZ2_MODULI[l]);
+  // k 2^(pa+pb) <= (M/2)(1 - 2^-30): the CRT rounding of q stays exact.
+  const long double room = log2m - 1.0L - log2l((long double)(k > 0 ? k : 1)) - 1e-6L;
+  const int total = (int)floorl(room);
+  if (total < 16) return b200_set_error(B200_EINVAL, "ozaki2: too few moduli for this k");
+  *pa = std::min(pmax, (total + 1) / 2);
+  *pb = std::min(pmax, total - *pa);
+  mod->n = N;
+  memset(crt, 0, sizeof *crt);
+  crt->bits = *pa + *pb;
+  const u128 mask42 = (((u128)1) << 42) - 1;
+  auto level = [&](u128 x, int lev) -> double {
+    const int shift = 84 - 42 * lev;
+    return ldexp((double)(unsigned long long)((x >> shift) & mask42), shift);
+  };
+  for (int l = 0; l < N; ++l) {
+    const int m = OZ2_MODULI[l];
+    mod->m[l] = crt->m[l] = m;
+    mod->c16[l] = crt->c16[l] = (int)((1u << 16) % (unsigned)m);
+    mod->c32[l] = (int)((((u128)1) << 32) % (u128)m);
+    mod->c48[l] = (int)((((u128)1) << 48) % (u128)m);
+    mod->magic[l] = crt->magic[l] = (int)((1ull << 32) / (unsigned long long)m + 1);
+    const u128 Ml = M / (u128)m;
+    const int r = (int)(Ml % (u128)m);
+    int y = 1;
+    while ((r * y) % m != 1) ++y;  // m <= 256: a direct search is enough
+    const u128 W = Ml * (u128)y;  // < M
+    for (int lev = 0; lev < 3; ++lev) crt->w[l][lev] = level(W, lev);
+  }
+  for (int lev = 0; lev < 3; ++lev) crt->mlev[lev] = level(M, lev);
+  crt->inv_m = (double)(1.0L / (long double)M);
+  return B200_OK;
+}
+
 }  // namespace
 
-int tc_run_ozaki(const b200_l3_desc_t *d) {
-  if (d->dtype != B200_F64) return b200_set_error(B200_EINVAL, "ozaki form is FP64-only");
+namespace {
+
+template <typename T>
+int run_ozaki(const b200_l3_desc_t *d, bool mod) {
   using C = OzCfg;
-  int slices = d->slices > 0 ? d->slices : b200_get_default_slices();
-  if (slices <= 0) slices = 7;
-  if (slices < 2 || slices > OZ_MAX_SLICES)
+  constexpr bool F64 = sizeof(T) == 8;
+  int slices = d->slices > 0 ? d->slices : b200_get_default_slices(d->dtype);
+  if (slices <= 0) slices = mod ? (F64 ? B200_MAX_MODULI : 8) : 7;
+  if (!mod && (slices < 2 || slices > OZ_MAX_SLICES))
     return b200_set_error(B200_EINVAL, "ozaki: slice count must be in [2, 12]");
+  if (mod && (slices < 6 || slices > B200_MAX_MODULI))
+    return b200_set_error(B200_EINVAL, "ozaki2: modulus count must be in [6, 16]");
   cudaStream_t s = b200_cur_stream();
   const long ktot = (long)d->k * d->npairs;
   const long mpad = b200_round_up(d->m, C::BM), npad = b200_round_up(d->n, C::BN);
   const long kpad = b200_round_up(ktot, C::BK);
   if (slices * (mpad > npad ? mpad : npad) > 0x7fffffffL)
     return b200_set_error(B200_EINVAL, "ozaki form: operand too large for 32-bit TMA rows");
+  OzParams p;
+  memset(&p, 0, sizeof p);
+  B200Moduli moduli;
+  memset(&moduli, 0, sizeof moduli);
+  int pa = 0, pb = 0;
+  // FP64 inputs carry 53 significant bits, FP32 inputs 24: a few bits more
+  // than that keeps elements a few binades below the row maximum exact.
+  if (mod) B200_TRY(oz2_setup(slices, ktot, F64 ? 56 : 27, &moduli, &p.crt, &pa, &pb));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   const int tiles = (int)((mpad / C::BM) * (npad / C::BN));
@@ -712,7 +905,9 @@ int tc_run_ozaki(const b200_l3_desc_t *d) {
   }
   if (st == B200_OK) st = b200_alloc(&ap, (size_t)slices * mpad * kpad);
   if (st == B200_OK) st = b200_alloc(&bp, (size_t)slices * npad * kpad);
-  if (st == B200_OK) st = b200_alloc(&work, sizeof(double) * grid * C::BM * C::BN);
+  const size_t work_bytes = mod ? (size_t)grid * slices * C::BM * C::BN
+                                : sizeof(double) * grid * C::BM * C::BN;
+  if (st == B200_OK) st = b200_alloc(&work, work_bytes);
   const mublis_l3_product_t &pr = d->product;
   PackView va[2], vb[2];
   for (int t = 0; t < d->npairs; ++t) {
@@ -723,23 +918,24 @@ int tc_run_ozaki(const b200_l3_desc_t *d) {
   }
   // Scales over the whole (concatenated) k of every row / column.
   for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
-    st = launch_absmax(va[t], false, d->m, d->k, (unsigned long long *)amax, s);
-    if (st == B200_OK) st = launch_absmax(vb[t], true, d->n, d->k, (unsigned long long *)bmax, s);
+    st = launch_absmax<T>(va[t], false, d->m, d->k, (unsigned long long *)amax, s);
+    if (st == B200_OK)
+      st = launch_absmax<T>(vb[t], true, d->n, d->k, (unsigned long long *)bmax, s);
   }
   for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
     long kk0 = (long)t * d->k, kk1 = t + 1 == d->npairs ? kpad : kk0 + d->k;
-    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, PACK_INT8_SLICES, slices,
-               (const unsigned long long *)amax};
-    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, PACK_INT8_SLICES, slices,
-               (const unsigned long long *)bmax};
-    st = launch_pack<double>(va[t], false, d->m, d->k, mpad, kk0, kk1, oa, s);
-    if (st == B200_OK) st = launch_pack<double>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
+    const int xform = mod ? PACK_INT8_MODULI : PACK_INT8_SLICES;
+    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, xform, slices,
+               (const unsigned long long *)amax, pa, moduli};
+    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, xform, slices,
+               (const unsigned long long *)bmax, pb, moduli};
+    st = launch_pack<T>(va[t], false, d->m, d->k, mpad, kk0, kk1, oa, s);
+    if (st == B200_OK) st = launch_pack<T>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
   }
   CUtensorMap ta, tb;
   if (st == B200_OK) st = b200_make_tmap(&ta, ap, 0, kpad, slices * mpad, C::BK, C::BM, 128);
   if (st == B200_OK) st = b200_make_tmap(&tb, bp, 0, kpad, slices * npad, C::BK, C::BN, 128);
   if (st == B200_OK) {
-    OzParams p;
     p.w.tiles_m = (int)(mpad / C::BM);
     p.w.tiles_n = (int)(npad / C::BN);
     p.w.bm = C::BM;
@@ -757,23 +953,27 @@ int tc_run_ozaki(const b200_l3_desc_t *d) {
     p.slices = slices;
     p.alpha = d->alpha;
     p.beta = d->beta;
-    p.c = (double *)d->c;
+    p.c = d->c;
     p.rs_c = d->rs_c;
     p.cs_c = d->cs_c;
-    p.work = (double *)work;
+    p.work = work;
     p.amax = (const unsigned long long *)amax;
     p.bmax = (const unsigned long long *)bmax;
     p.err = b200_device_error_word();
-    static bool configured = false;
-    if (!configured) {
-      if (cudaFuncSetAttribute(tc_ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               C::SMEM) != cudaSuccess)
+    auto kern = tc_ozaki_kernel<true, T>;
+    if constexpr (F64) {
+      if (!mod) kern = tc_ozaki_kernel<false, double>;
+    }
+    static bool configured[2] = {false, false};
+    if (!configured[mod]) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) !=
+          cudaSuccess)
         st = b200_set_error(B200_ECUDA, "ozaki: smem attribute");
-      configured = st == B200_OK;
+      configured[mod] = st == B200_OK;
     }
     if (st == B200_OK) {
-      B200ProfScope prof("tc_ozaki_i8", s);
-      tc_ozaki_kernel<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);
+      B200ProfScope prof(mod ? (F64 ? "tc_ozaki2_i8" : "tc_ozaki2_s_i8") : "tc_ozaki_i8", s);
+      kern<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);
       if (cudaGetLastError() != cudaSuccess) st = b200_set_error(B200_ECUDA, "ozaki launch failed");
     }
   }
@@ -782,4 +982,13 @@ int tc_run_ozaki(const b200_l3_desc_t *d) {
   b200_free(work);
   b200_free(amax);
   return st;
+}
+
+}  // namespace
+
+int tc_run_ozaki(const b200_l3_desc_t *d) {
+  const bool mod = d->form == B200_FORM_OZAKI2;
+  if (d->dtype == B200_F64) return run_ozaki<double>(d, mod);
+  if (!mod) return b200_set_error(B200_EINVAL, "the slice Ozaki form is FP64-only");
+  return run_ozaki<float>(d, true);
 }

@@ -9,8 +9,13 @@ restatement, or against a double-double evaluation of sampled entries at
                                  element, not k-dependent)
   ozaki:8 (FP64)        4 * k * 2^-53                  (same as plain)
   ozaki:7 (FP64)        2^-44
+  ozaki2 (FP64, 16 moduli, ~55-bit inputs)   4 * k * 2^-53
+  ozaki2 (FP32, 8 moduli, ~25-bit inputs)    4 * k * 2^-24
+  ozaki2:14 (FP64, ~49-bit inputs at k=700)  2^-44
+  ozaki2:6 (FP64, ~18-bit inputs: checks the CRT with M < 2^84)  2^-14
 The 8192^3 study also checks the headline claims: bf16x6 has the error of
-plain FP32 (within 1.5x) and ozaki:8 has at most the error of plain FP64.
+plain FP32 (within 1.5x), and ozaki:8 and ozaki2 have at most the error of
+plain FP64.
 Run with -s to print the measured table.
 """
 import ctypes
@@ -30,6 +35,9 @@ TOL = {
     "bf16x3": lambda k, u: 2.0 ** -15,
     "ozaki:8": lambda k, u: 4 * k * 2.0 ** -53,
     "ozaki:7": lambda k, u: 2.0 ** -44,
+    "ozaki2": lambda k, u: 4 * k * 2.0 ** -53,
+    "ozaki2:14": lambda k, u: 2.0 ** -44,
+    "ozaki2:6": lambda k, u: 2.0 ** -14,
 }
 
 
@@ -63,7 +71,7 @@ FAMILY = [("gemm", dict(ta=False, tb=False)), ("gemm", dict(ta=True, tb=True)),
           ("trsm", dict(right=False, lower=True, ta=False, unit=False))]
 
 
-@pytest.mark.parametrize("form", ["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("form", ["bf16x3", "bf16x6", "ozaki2"])
 @pytest.mark.parametrize("routine,flags", FAMILY, ids=[f"{r}{i}" for i, (r, _) in enumerate(FAMILY)])
 def test_fp32_tensor_forms(lib, form, routine, flags):
     case = dict(routine=routine, dtype="float32", order="F", m=640, n=544, k=704, alpha=0.75,
@@ -75,7 +83,7 @@ def test_fp32_tensor_forms(lib, form, routine, flags):
     assert err <= TOL[form](cs.inner_dim(case), 2.0 ** -24), err
 
 
-@pytest.mark.parametrize("form", ["ozaki:7", "ozaki:8"])
+@pytest.mark.parametrize("form", ["ozaki:7", "ozaki:8", "ozaki2", "ozaki2:14", "ozaki2:6"])
 @pytest.mark.parametrize("routine,flags", FAMILY, ids=[f"{r}{i}" for i, (r, _) in enumerate(FAMILY)])
 def test_fp64_ozaki(lib, form, routine, flags):
     case = dict(routine=routine, dtype="float64", order="F", m=600, n=520, k=680, alpha=0.75,
@@ -107,7 +115,7 @@ def test_wide_range_inputs_ozaki(lib):
     exact = hi + lo
     den = np.linalg.norm(a) * np.linalg.norm(b)
     errs = {}
-    for form in ("plain", "ozaki:8"):
+    for form in ("plain", "ozaki:8", "ozaki2"):
         assert lib.mublis_b200_set_form(b"d", form.encode()) == 0
         c = np.zeros((n, n), order="F")
         assert lib.mublis_dgemm(0, 0, n, n, n, 1.0, a.ctypes.data, 1, n, b.ctypes.data, 1, n,
@@ -116,6 +124,30 @@ def test_wide_range_inputs_ozaki(lib):
         errs[form] = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
     lib.mublis_b200_set_form(b"d", b"plain")
     assert errs["ozaki:8"] <= max(errs["plain"], 4 * n * 2.0 ** -53), errs
+    assert errs["ozaki2"] <= max(errs["plain"], 4 * n * 2.0 ** -53), errs
+
+
+@pytest.mark.parametrize("form", ["ozaki:8", "ozaki2"])
+def test_ozaki_long_k_chunks(lib, form):
+    """k = 70001 spans several exact-int32 chunks of both integer forms
+    (8192 for slices, 65536 for moduli): the per-chunk partial results must
+    combine to the double-double value of sampled entries."""
+    m, n, k = 200, 136, 70001
+    a = orc.fill(m, k, np.float64, 9, 0)
+    b = orc.fill(k, n, np.float64, 9, 1)
+    c0 = orc.fill(m, n, np.float64, 9, 2)
+    rng = np.random.default_rng(5)
+    rows, cols = rng.integers(0, m, 256), rng.integers(0, n, 256)
+    hi, lo = orc.dd_gemm_entries(a, b, rows, cols, alpha=0.75, beta=0.25, c0=c0)
+    assert lib.mublis_b200_set_form(b"d", form.encode()) == 0
+    c = c0.copy(order="F")
+    assert lib.mublis_dgemm(0, 0, m, n, k, 0.75, a.ctypes.data, 1, m, b.ctypes.data, 1, k,
+                            0.25, c.ctypes.data, 1, m) == 0, mb.last_error(lib)
+    lib.mublis_b200_set_form(b"d", b"plain")
+    d = c[rows, cols] - (hi + lo)
+    den = 0.75 * np.linalg.norm(a) * np.linalg.norm(b) + 0.25 * np.linalg.norm(c0)
+    err = np.sqrt((d ** 2).sum() * m * n / len(rows)) / den
+    assert err <= 4 * k * 2.0 ** -53, err
 
 
 def _device_matrix(torch, lib, p, n, seed, mid, kind=0):
@@ -136,7 +168,7 @@ def test_precision_study_8192(lib, kind):
     rng = np.random.default_rng(7)
     rows, cols = rng.integers(0, n, ns), rng.integers(0, n, ns)
     table = {}
-    for p, forms in (("s", ["plain", "bf16x3", "bf16x6"]), ("d", ["plain", "ozaki:7", "ozaki:8"])):
+    for p, forms in (("s", ["plain", "bf16x3", "bf16x6", "ozaki2"]), ("d", ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
         a, b, c0 = (_device_matrix(torch, lib, p, n, 0, i, kind) for i in range(3))
         ah, bh, ch = (np.asfortranarray(x.cpu().numpy().T) for x in (a, b, c0))
         hi, lo = orc.dd_gemm_entries(ah, bh, rows, cols, alpha=1.0, beta=0.5, c0=ch)
@@ -163,5 +195,7 @@ def test_precision_study_8192(lib, kind):
         print(f"  {key:14s} {nw:.3e}  {mx:.3e}")
     assert table["sgemm bf16x6"][0] <= 1.5 * table["sgemm plain"][0]
     assert table["dgemm ozaki:8"][0] <= table["dgemm plain"][0]
+    assert table["dgemm ozaki2"][0] <= table["dgemm plain"][0]
+    assert table["sgemm ozaki2"][0] <= table["sgemm plain"][0]
     assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
     assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)
