@@ -308,6 +308,32 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
         lib.mublis_b200_set_form(p.encode(), b"plain")
         del a, b, c
         torch.cuda.empty_cache()
+    # DTRSM of order n with n right-hand sides: FP64 diagonal blocks, updates
+    # plain or emulated (left, lower, non-unit; A = U[-1,1)/n off the
+    # diagonal, U[1,2) on it).
+    a = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    dg = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    b = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    lib.mublis_b200_fill_d(ctypes.c_void_p(a.data_ptr()), n, n, n, 0, 0, 0)
+    lib.mublis_b200_fill_d(ctypes.c_void_p(dg.data_ptr()), n, n, n, 0, 9, 2)
+    lib.mublis_b200_fill_d(ctypes.c_void_p(b.data_ptr()), n, n, n, 0, 1, 0)
+    a.div_(n)
+    a.diagonal().copy_(dg.diagonal())
+    del dg
+    b0 = b.clone()
+    for f in ("plain", "ozaki2"):
+        lib.mublis_b200_set_form(b"d", f.encode())
+        call = lambda: lib.cblas_dtrsm(COL, LEFT, LOWER, NT, NONUNIT, n, n, 1.0,  # noqa: E731
+                                       ctypes.c_void_p(a.data_ptr()), n,
+                                       ctypes.c_void_p(b.data_ptr()), n)
+        call()
+        b.copy_(b0)
+        ms = timed(torch, call, 2)
+        b.copy_(b0)
+        out[f"dtrsm_{n}_{f}"] = round(float(n) ** 3 / ms / 1e9, 2)
+    lib.mublis_b200_set_form(b"d", b"plain")
+    del a, b, b0
+    torch.cuda.empty_cache()
     return out
 
 
@@ -500,7 +526,7 @@ def served_study(torch, lib, nreq: int = 400) -> dict:
                 "served": {"tflops": round(tot / span_v / 1e12, 2), "p50_ms": pct(lat_v, 50),
                            "p99_ms": pct(lat_v, 99), "batches": int(st.batches),
                            "batched_requests": int(st.batched_requests),
-                           "forms": "auto (bf16x6 / ozaki:8 above crossover, else plain)"},
+                           "forms": "auto (bf16x6 / ozaki2 above crossover, else plain)"},
                 "serialized_plain": {"tflops": round(tot / span_s / 1e12, 2),
                                      "p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99)},
                 "throughput_ratio": round(span_s / span_v, 2)}

@@ -72,9 +72,10 @@ struct PackOut {
   B200Moduli mod;                    // PACK_INT8_MODULI
 };
 
-// Symmetric residue of t modulo m in [-128, 127] (m <= 256, |t| < 2^26).
-// q = mulhi(t, floor(2^32/m) + 1) is floor(t/m) up to +-1 for |t| < 2^26,
-// so r = t - q m lies in [-m, 2m) and two conditional corrections bring it
+// Symmetric residue of t modulo m in [-128, 127] (m <= 256, any int32 t).
+// With magic = floor(2^32/m) + 1 = 2^32/m + d, 0 < d <= 1, mulhi(t, magic)
+// = floor(t/m + e) with |e| = |t| d / 2^32 < 1/2, so it is floor(t/m) up to
+// +-1; r = t - q m lies in [-m, 2m) and two conditional corrections bring it
 // to [0, m) before it is centred.
 __device__ __forceinline__ int b200_sym_mod(int t, int m, int magic) {
   int r = t - __mulhi(t, magic) * m;

@@ -18,18 +18,20 @@
 namespace {
 
 // "auto" picks, per call, the fastest form whose error is no worse than the
-// plain kernel's: the tensor-core forms pay a split/slice pass and, for
-// Ozaki, s(s+1)/2 products, so below these sizes (crossovers measured on
-// B200) plain wins.  FP32: BF16x6 (3-term split, error equal to plain FP32)
-// when min(m, n) and k are >= 512.  FP64: Ozaki with 8 slices (error below
-// plain FP64) when min(m, n) and k are >= 4096.
+// plain kernel's: the tensor-core forms pay a split/residue pass and, for
+// the integer forms, one int8 product per modulus, so below these sizes
+// (crossovers measured on B200) plain wins.  FP32: BF16x6 (3-term split,
+// error equal to plain FP32) when min(m, n) and k are >= 512.  FP64: the
+// modular Ozaki form with 16 moduli (error ~36x below plain FP64) when
+// min(m, n) and k are >= 4096 (at 2048^3 plain is faster, at 4096^3 the
+// modular form is 1.8x plain, at 8192^3 2.9x).
 int resolve_form(const b200_l3_desc_t *d) {
   int f = d->form == B200_FORM_AUTO ? b200_get_default_form(d->dtype) : d->form;
   if (f == B200_FORM_POLICY) {
     const long m = d->m, n = d->n, k = (long)d->k * d->npairs;
     const long mn = m < n ? m : n;
     if (d->dtype == B200_F32) return mn >= 512 && k >= 512 ? B200_FORM_BF16X6 : B200_FORM_PLAIN;
-    return mn >= 4096 && k >= 4096 ? B200_FORM_OZAKI : B200_FORM_PLAIN;
+    return mn >= 4096 && k >= 4096 ? B200_FORM_OZAKI2 : B200_FORM_PLAIN;
   }
   if (d->dtype == B200_F32 && f == B200_FORM_OZAKI) f = B200_FORM_PLAIN;
   if (d->dtype == B200_F64 && (f == B200_FORM_BF16X3 || f == B200_FORM_BF16X6)) f = B200_FORM_PLAIN;

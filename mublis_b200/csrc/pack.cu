@@ -135,6 +135,110 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
   }
 }
 
+// K-major panels (the tensor-core forms): a CTA covers 32 rows (mn) x 64 k.
+// Each thread turns 8 consecutive k of one row into every output plane and
+// writes them as one vector per plane (16 bytes of bf16, 8 bytes of int8,
+// 32/64 bytes of T), so a warp writes 4 rows x 128 contiguous bytes of bf16
+// per plane instead of 2-byte scattered stores.  Requires kk0 and the
+// panel's row pitch to be multiples of 8 (every K-major panel is padded to
+// the MMA k-block).
+template <typename T>
+__device__ __forceinline__ void kmajor_store8(const PackOut &o, long mn, long off, const T (&v)[8]) {
+  if (o.xform == PACK_BF16_SPLIT) {
+    __nv_bfloat16 *out = (__nv_bfloat16 *)o.out;
+    __align__(16) __nv_bfloat16 h[8], l[8], l2[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float f = (float)v[j];
+      h[j] = __float2bfloat16_rn(f);
+      const float r1 = f - __bfloat162float(h[j]);
+      l[j] = __float2bfloat16_rn(r1);
+      l2[j] = __float2bfloat16_rn(r1 - __bfloat162float(l[j]));
+    }
+    *reinterpret_cast<uint4 *>(out + off) = *reinterpret_cast<const uint4 *>(h);
+    *reinterpret_cast<uint4 *>(out + off + o.plane_stride) = *reinterpret_cast<const uint4 *>(l);
+    if (o.terms > 2)
+      *reinterpret_cast<uint4 *>(out + off + 2 * o.plane_stride) =
+          *reinterpret_cast<const uint4 *>(l2);
+  } else if (o.xform == PACK_INT8_MODULI) {
+    int8_t *out = (int8_t *)o.out;
+    const int sh = o.bits - b200_scale_exp(o.absmax[mn]);
+    int hh[8], hl[8], lh[8], ll[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double x = rint(ldexp((double)v[j], sh));
+      const double dh = floor(x * 0x1p-48), x1 = fma(-dh, 0x1p48, x);
+      const double dl = floor(x1 * 0x1p-32), x2 = fma(-dl, 0x1p32, x1);
+      const double d3 = floor(x2 * 0x1p-16);
+      hh[j] = (int)dh, hl[j] = (int)dl, lh[j] = (int)d3, ll[j] = (int)fma(-d3, 0x1p16, x2);
+    }
+#pragma unroll
+    for (int t = 0; t < B200_MAX_MODULI; ++t) {
+      if (t >= o.terms) break;
+      uint32_t w[2] = {0, 0};
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int r = b200_sym_mod(hh[j] * o.mod.c48[t] + hl[j] * o.mod.c32[t] +
+                                       lh[j] * o.mod.c16[t] + ll[j],
+                                   o.mod.m[t], o.mod.magic[t]);
+        w[j >> 2] |= (uint32_t)(r & 0xff) << (8 * (j & 3));
+      }
+      *reinterpret_cast<uint2 *>(out + off + t * o.plane_stride) = make_uint2(w[0], w[1]);
+    }
+  } else if (o.xform == PACK_INT8_SLICES) {
+    int8_t *out = (int8_t *)o.out;
+    const int sh = 7 - b200_scale_exp(o.absmax[mn]);
+    double r[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = ldexp((double)v[j], sh);
+    for (int t = 0; t < o.terms; ++t) {
+      uint32_t w[2] = {0, 0};
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double q = trunc(r[j]);
+        w[j >> 2] |= (uint32_t)((int)q & 0xff) << (8 * (j & 3));
+        r[j] = (r[j] - q) * 128.0;
+      }
+      *reinterpret_cast<uint2 *>(out + off + t * o.plane_stride) = make_uint2(w[0], w[1]);
+    }
+  } else {
+    T *out = (T *)o.out + off;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = v[j];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) pack_kmajor_kernel(PackView v, bool b_side, long mn_len,
+                                                          long k_len, long kk0, long kk1,
+                                                          PackOut o, bool mn_fast_load) {
+  __shared__ T tile[64][33];  // [kk_local][mn_local]
+  const int tid = threadIdx.x;
+  const long mn_base = (long)blockIdx.x * 32;
+  const long kk_base = kk0 + (long)blockIdx.y * 64;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int e = tid + 256 * q;  // 2048 elements
+    const int mn_l = mn_fast_load ? e & 31 : e >> 6;
+    const int kk_l = mn_fast_load ? e >> 5 : e & 63;
+    const long mn = mn_base + mn_l, kk = kk_base + kk_l, kl = kk - kk0;
+    T val = T(0);
+    if (mn < mn_len && kl < k_len && kk < kk1) {
+      const long r = b_side ? kl : mn, c = b_side ? mn : kl;
+      val = load_logical<T>(v, r, c);
+    }
+    tile[kk_l][mn_l] = val;
+  }
+  __syncthreads();
+  const int mn_l = tid >> 3, kc = (tid & 7) * 8;
+  const long mn = mn_base + mn_l, kk = kk_base + kc;
+  if (kk >= kk1) return;
+  T vals[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) vals[j] = tile[kc + j][mn_l];
+  kmajor_store8<T>(o, mn, mn * o.ld + kk, vals);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) absmax_kernel(PackView v, bool b_side, long mn_len,
                                                      long k_len, bool mn_fast_load,
@@ -189,9 +293,17 @@ int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn
   long mn_stride = b_side ? v.cs : v.rs;
   long kk_stride = b_side ? v.rs : v.cs;
   bool mn_fast = labs(mn_stride) <= labs(kk_stride);
+  B200ProfScope prof("pack", s);
+  if (o.layout == PACK_K_MAJOR && mn_pad % 32 == 0 && kk0 % 8 == 0 && (kk1 - kk0) % 8 == 0 &&
+      o.ld % 8 == 0) {
+    dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 64));
+    if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
+    pack_kmajor_kernel<T><<<grid, 256, 0, s>>>(v, b_side, mn_len, k_len, kk0, kk1, o, mn_fast);
+    B200_LAUNCH_CHECK();
+    return B200_OK;
+  }
   dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 32));
   if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
-  B200ProfScope prof("pack", s);
   pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, kk0, kk1, o, mn_fast);
   B200_LAUNCH_CHECK();
   return B200_OK;

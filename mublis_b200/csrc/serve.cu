@@ -121,7 +121,7 @@ size_t scratch_estimate(const Req &r) {
   size_t mp = b200_round_up(d.m, 256), np = b200_round_up(d.n, 256);
   size_t kp = b200_round_up((long)d.k * d.npairs, 128);
   int f = d.form;
-  if (f == B200_FORM_POLICY) f = r.dtype == B200_F64 ? B200_FORM_OZAKI : B200_FORM_BF16X6;
+  if (f == B200_FORM_POLICY) f = r.dtype == B200_F64 ? B200_FORM_OZAKI2 : B200_FORM_BF16X6;
   if (f == B200_FORM_BF16X6) return 3 * (mp + np) * kp * 2;
   if (f == B200_FORM_BF16X3) return 2 * (mp + np) * kp * 2;
   if (f == B200_FORM_OZAKI) return 12 * (mp + np) * kp + 148 * 256 * 256 * 8;

@@ -8,29 +8,37 @@
 //   * recursive halving: solve the top half, update the bottom half with one
 //     GEMM (k = half the order, so it runs at GEMM speed), solve the bottom
 //     half (upper: mirror image);
-//   * leaves are the 64 x 64 diagonal blocks.  All of them are inverted up
-//     front in one launch (trsm_inv_diag_kernel: substitution against the
-//     reciprocal diagonal, computed once and multiplied -- never divided --
-//     as the reference does; the unstored triangle and a unit diagonal are
-//     never read), so each leaf solve is X_b = inv(A_bb) B_b, a parallel
-//     64 x n GEMM instead of a 64-deep dependent chain per column;
-//   * updates and leaf products with k <= 256 read their operands directly
-//     (no pack pass); larger ones use the packed driver path;
+//   * leaves are the 256 x 256 diagonal blocks, inverted up front: one launch
+//     inverts every 64 x 64 diagonal block by substitution against the
+//     reciprocal diagonal (computed once and multiplied -- never divided --
+//     as the reference does), then two doubling steps of two batched
+//     (grouped) GEMM launches each build the 128- and 256-blocks,
+//     inv([A11 0; A21 A22]) = [inv11 0; -inv22 A21 inv11  inv22];
+//   * each leaf solve is then X_b = inv(A_bb) B_b, one 256-deep GEMM over all
+//     right-hand sides (plain FP64/FP32: the diagonal blocks never use an
+//     emulated form), and every update is a GEMM of k >= 256 on the packed
+//     path (and the caller's form);
 //   * the unit diagonal and the unstored triangle are never read.
 // alpha is applied once up front (the reference's alpha_eff on the first
 // block, trsm.c:96-97).
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "kernels.cuh"
 
 namespace {
 
-constexpr int LEAF = 64;  // rows per diagonal block (leaf)
+constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
+constexpr int BIG = 256;  // inverted diagonal blocks the solve uses (leaves)
+constexpr int PER_BIG = BIG / LEAF;
 
-// One CTA per diagonal block: thread j computes column j of the inverse of
-// the block's (lower or upper) triangle by substitution, L x = e_j.  Rows
-// past the matrix order are padded with the identity.  Output: block b as a
-// LEAF x LEAF column-major matrix at inv + b * LEAF * LEAF.
+// One CTA per LEAF block: thread j computes column j of the inverse of the
+// block's (lower or upper) triangle by substitution, L x = e_j.  Rows past
+// the matrix order are padded with the identity.  Output: big block
+// b / PER_BIG is a BIG x BIG column-major matrix at inv + (b / PER_BIG) *
+// BIG * BIG (zeroed beforehand); LEAF block b lands on its diagonal at
+// offset (b % PER_BIG) * LEAF.
 template <typename T>
 __global__ void __launch_bounds__(LEAF) trsm_inv_diag_kernel(int m, const T *a, long rs_a,
                                                               long cs_a, bool lower, bool unit,
@@ -72,7 +80,8 @@ __global__ void __launch_bounds__(LEAF) trsm_inv_diag_kernel(int m, const T *a, 
       x[i] = r * L[i][i];
     }
   }
-  T *out = inv + (size_t)b * LEAF * LEAF + (size_t)j * LEAF;
+  const size_t off = (size_t)(b % PER_BIG) * LEAF;
+  T *out = inv + (size_t)(b / PER_BIG) * BIG * BIG + off * (BIG + 1) + (size_t)j * BIG;
 #pragma unroll
   for (int i = 0; i < LEAF; ++i) out[i] = x[i];
 }
@@ -105,35 +114,91 @@ b200_l3_desc_t plain_gemm_desc(int dtype, int form, int slices) {
   return g;
 }
 
+// Doubling: with the inverses of the h-blocks on the diagonal of every big
+// block, fill in the off-diagonal h x h block of every 2h-block:
+//   lower  X21 = -inv22 (A21 inv11),   upper  X12 = -inv11 (A12 inv22),
+// as two grouped launches (the products into `tmp`, then into `inv`).  A
+// pair whose second half is cut by the matrix order uses only its valid
+// m2 rows/columns; the identity padding makes the rest already correct.
+template <typename T>
+int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, cudaStream_t s) {
+  const T *a = (const T *)d->a;
+  const bool lower = d->uplo == MUBLIS_LOWER;
+  const long m = d->m;
+  for (long h = LEAF; h < BIG; h *= 2) {
+    std::vector<b200_l3_desc_t> g1, g2;
+    for (long r0 = 0; r0 + h < m; r0 += 2 * h) {
+      const int m2 = (int)std::min(h, m - r0 - h);
+      T *blk = inv + (r0 / BIG) * BIG * BIG;
+      const long o1 = r0 % BIG, o2 = o1 + h;
+      const T *inv11 = blk + o1 * (BIG + 1), *inv22 = blk + o2 * (BIG + 1);
+      T *t = tmp + (r0 / (2 * h)) * h * h;
+      b200_l3_desc_t p = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
+      b200_l3_desc_t q = p;
+      p.alpha = 1.0;
+      q.alpha = -1.0;
+      p.beta = q.beta = 0.0;
+      if (lower) {  // T (m2 x h) = A21 inv11;  X21 = -inv22[m2 x m2] T
+        p.m = m2, p.n = (int)h, p.k = (int)h;
+        p.a[0] = a + (r0 + h) * d->rs_a + r0 * d->cs_a, p.rs_a[0] = d->rs_a, p.cs_a[0] = d->cs_a;
+        p.b[0] = inv11, p.rs_b[0] = 1, p.cs_b[0] = BIG;
+        q.m = m2, q.n = (int)h, q.k = m2;
+        q.a[0] = inv22, q.rs_a[0] = 1, q.cs_a[0] = BIG;
+        q.c = blk + o2 + o1 * BIG;
+      } else {  // T (h x m2) = A12 inv22[m2 x m2];  X12 = -inv11 T
+        p.m = (int)h, p.n = m2, p.k = m2;
+        p.a[0] = a + r0 * d->rs_a + (r0 + h) * d->cs_a, p.rs_a[0] = d->rs_a, p.cs_a[0] = d->cs_a;
+        p.b[0] = inv22, p.rs_b[0] = 1, p.cs_b[0] = BIG;
+        q.m = (int)h, q.n = m2, q.k = (int)h;
+        q.a[0] = inv11, q.rs_a[0] = 1, q.cs_a[0] = BIG;
+        q.c = blk + o1 + o2 * BIG;
+      }
+      p.c = t, p.rs_c = 1, p.cs_c = h;
+      q.b[0] = t, q.rs_b[0] = 1, q.cs_b[0] = h;
+      q.rs_c = 1, q.cs_c = BIG;
+      g1.push_back(p);
+      g2.push_back(q);
+    }
+    if (g1.empty()) break;
+    std::vector<const b200_l3_desc_t *> p1, p2;
+    for (size_t i = 0; i < g1.size(); ++i) {
+      p1.push_back(&g1[i]);
+      p2.push_back(&g2[i]);
+    }
+    B200_TRY(b200_grouped_gemm_async(d->dtype, p1.data(), (int)p1.size(), s));
+    B200_TRY(b200_grouped_gemm_async(d->dtype, p2.data(), (int)p2.size(), s));
+  }
+  return B200_OK;
+}
+
 template <typename T>
 int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   const T *a = (const T *)d->a;
   T *b = (T *)d->b;
   const bool lower = d->uplo == MUBLIS_LOWER;
   long rows = r1 - r0;
-  if (rows <= LEAF) {
-    // X_b = inv(A_bb) B_b, in place: every CTA of the direct kernel covers
-    // all rows of the leaf for its columns (tile height >= LEAF), so it reads
-    // its B columns completely before it writes them, and CTAs own disjoint
-    // columns.
+  if (rows <= BIG) {
+    // X_b = inv(A_bb) B_b in place: the packed path packs B_b before the
+    // product writes it.  Plain precision: the diagonal-block solve is FP64
+    // (FP32) whatever form the updates use.
     b200_l3_desc_t g = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
     g.m = (int)rows;
     g.n = d->n;
     g.k = (int)rows;
     g.alpha = 1.0;
     g.beta = 0.0;
-    g.a[0] = inv + (r0 / LEAF) * LEAF * LEAF;
+    g.a[0] = inv + (r0 / BIG) * BIG * BIG;
     g.rs_a[0] = 1;
-    g.cs_a[0] = LEAF;
+    g.cs_a[0] = BIG;
     g.b[0] = b + r0 * d->rs_b;
     g.rs_b[0] = d->rs_b;
     g.cs_b[0] = d->cs_b;
     g.c = b + r0 * d->rs_b;
     g.rs_c = d->rs_b;
     g.cs_c = d->cs_b;
-    return b200_gemm_direct_min_rows(&g, LEAF);
+    return b200_l3_run(&g);
   }
-  long half = b200_round_up((rows + 1) / 2, LEAF);
+  long half = b200_round_up((rows + 1) / 2, BIG);
   long mid = r0 + half;
   // Rows solved first (src) and rows updated by them (dst).
   long s0 = lower ? r0 : mid, s1 = lower ? mid : r1;
@@ -154,21 +219,25 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   g.c = b + t0 * d->rs_b;
   g.rs_c = d->rs_b;
   g.cs_c = d->cs_b;
-  // Thin updates (small k) read their operands directly; thick ones go
-  // through the packed driver path (and the tensor-core forms).
-  B200_TRY(g.k <= 256 ? b200_gemm_direct(&g) : b200_l3_run(&g));
+  B200_TRY(b200_l3_run(&g));
   return trsm_rec<T>(d, inv, t0, t1);
 }
 
 template <typename T>
 int trsm_solve(const b200_trsm_desc_t *d) {
   cudaStream_t s = b200_cur_stream();
-  T *inv = nullptr;
-  const long blocks = b200_ceil_div(d->m, LEAF);
-  B200_TRY(b200_alloc((void **)&inv, sizeof(T) * blocks * LEAF * LEAF));
-  int st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
-                              d->unit_diag != 0, inv, s);
+  T *inv = nullptr, *tmp = nullptr;
+  const long bigs = b200_ceil_div(d->m, BIG);
+  B200_TRY(b200_alloc((void **)&inv, sizeof(T) * bigs * BIG * BIG));
+  int st = b200_alloc((void **)&tmp, sizeof(T) * bigs * BIG * BIG / 2);
+  if (st == B200_OK && cudaMemsetAsync(inv, 0, sizeof(T) * bigs * BIG * BIG, s) != cudaSuccess)
+    st = b200_set_error(B200_ECUDA, "trsm: memset failed");
+  if (st == B200_OK)
+    st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
+                            d->unit_diag != 0, inv, s);
+  if (st == B200_OK) st = grow_inverse<T>(d, inv, tmp, s);
   if (st == B200_OK) st = trsm_rec<T>(d, inv, 0, d->m);
+  b200_free(tmp);
   b200_free(inv);
   return st;
 }

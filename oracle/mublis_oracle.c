@@ -321,20 +321,34 @@ void oracle_dd_gemm_entries(int is_f32, int ta, int tb, long k, double alpha, co
                             long lda, const void *b, long ldb, double beta, const void *c0,
                             long ldc, long count, const long *rows, const long *cols,
                             double *hi, double *lo) {
-  for (long q = 0; q < count; ++q) {
-    long i = rows[q], j = cols[q];
-    double s = 0, e = 0;
-    for (long p = 0; p < k; ++p) {
-      long ia = ta ? p + i * lda : i + p * lda;
-      long ib = tb ? j + p * ldb : p + j * ldb;
-      double x = is_f32 ? (double)((const float *)a)[ia] : ((const double *)a)[ia];
-      double y = is_f32 ? (double)((const float *)b)[ib] : ((const double *)b)[ib];
-      double ph = x * y, pl = fma(x, y, -ph);
-      double t, te;
-      two_sum(s, ph, &t, &te);
-      s = t;
-      e += te + pl;
+  /* Four entries at a time: their compensated sums are independent chains,
+   * so interleaving them hides the latency of each chain's two_sum. */
+  for (long q0 = 0; q0 < count; q0 += 4) {
+    const int nq = count - q0 < 4 ? (int)(count - q0) : 4;
+    double s4[4] = {0, 0, 0, 0}, e4[4] = {0, 0, 0, 0};
+    long ia0[4], ias[4], ib0[4], ibs[4];
+    for (int u = 0; u < 4; ++u) {
+      long i = rows[q0 + (u < nq ? u : 0)], j = cols[q0 + (u < nq ? u : 0)];
+      ia0[u] = ta ? i * lda : i;
+      ias[u] = ta ? 1 : lda;
+      ib0[u] = tb ? j : j * ldb;
+      ibs[u] = tb ? ldb : 1;
     }
+    for (long p = 0; p < k; ++p) {
+      for (int u = 0; u < 4; ++u) {
+        long ia = ia0[u] + p * ias[u], ib = ib0[u] + p * ibs[u];
+        double x = is_f32 ? (double)((const float *)a)[ia] : ((const double *)a)[ia];
+        double y = is_f32 ? (double)((const float *)b)[ib] : ((const double *)b)[ib];
+        double ph = x * y, pl = fma(x, y, -ph);
+        double t, te;
+        two_sum(s4[u], ph, &t, &te);
+        s4[u] = t;
+        e4[u] += te + pl;
+      }
+    }
+    for (int u = 0; u < nq; ++u) {
+    const long q = q0 + u, i = rows[q], j = cols[q];
+    const double s = s4[u], e = e4[u];
     /* alpha * (s + e) + beta * c, still compensated */
     double ah = alpha * s, al = fma(alpha, s, -ah) + alpha * e;
     double rh = ah, rl = al;
@@ -350,5 +364,6 @@ void oracle_dd_gemm_entries(int is_f32, int ta, int tb, long k, double alpha, co
     two_sum(rh, rl, &t, &te);
     hi[q] = t;
     lo[q] = te;
+    }
   }
 }

@@ -16,6 +16,7 @@ use this module, and only as the thing the B200 library is checked against.
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
@@ -150,9 +151,12 @@ def trsm_matrix(n: int, dtype, seed: int, matrix_id: int) -> np.ndarray:
     return np.asfortranarray(a.astype(dtype))
 
 
-def dd_gemm_entries(a, b, rows, cols, alpha=1.0, beta=0.0, c0=None, ta=False, tb=False):
+def dd_gemm_entries(a, b, rows, cols, alpha=1.0, beta=0.0, c0=None, ta=False, tb=False,
+                    threads=None):
     """Double-double values of selected entries of alpha*op(A)op(B)+beta*C0
-    (A, B, C0 column-major float32/float64); returns (hi, lo) arrays."""
+    (A, B, C0 column-major float32/float64); returns (hi, lo) arrays.  The
+    entries are split over `threads` host threads (default: all cores); the
+    C routine runs without the GIL."""
     a = np.asfortranarray(a)
     b = np.asfortranarray(b)
     rows = np.ascontiguousarray(rows, dtype=np.int64)
@@ -165,8 +169,22 @@ def dd_gemm_entries(a, b, rows, cols, alpha=1.0, beta=0.0, c0=None, ta=False, tb
     if c0 is not None and beta != 0:
         c0 = np.asfortranarray(c0)
         cptr, ldc = c0.ctypes.data, c0.shape[0]
-    restated().oracle_dd_gemm_entries(is32, int(ta), int(tb), k, alpha, a.ctypes.data,
-                                      a.shape[0], b.ctypes.data, b.shape[0], beta, cptr, ldc,
-                                      len(rows), rows.ctypes.data, cols.ctypes.data,
-                                      hi.ctypes.data, lo.ctypes.data)
+    fn = restated().oracle_dd_gemm_entries
+    count = len(rows)
+    nt = max(1, min(threads or os.cpu_count() or 1, count // 64 or 1))
+    bounds = [count * t // nt for t in range(nt + 1)]
+
+    def part(t):
+        q0, q1 = bounds[t], bounds[t + 1]
+        if q1 > q0:
+            fn(is32, int(ta), int(tb), k, alpha, a.ctypes.data, a.shape[0], b.ctypes.data,
+               b.shape[0], beta, cptr, ldc, q1 - q0, rows.ctypes.data + 8 * q0,
+               cols.ctypes.data + 8 * q0, hi.ctypes.data + 8 * q0, lo.ctypes.data + 8 * q0)
+
+    if nt == 1:
+        part(0)
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(nt) as ex:
+            list(ex.map(part, range(nt)))
     return hi, lo

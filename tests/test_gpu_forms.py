@@ -35,7 +35,7 @@ TOL = {
     "bf16x3": lambda k, u: 2.0 ** -15,
     "ozaki:8": lambda k, u: 4 * k * 2.0 ** -53,
     "ozaki:7": lambda k, u: 2.0 ** -44,
-    "ozaki2": lambda k, u: 4 * k * 2.0 ** -53,
+    "ozaki2": lambda k, u: 4 * k * u,
     "ozaki2:14": lambda k, u: 2.0 ** -44,
     "ozaki2:6": lambda k, u: 2.0 ** -14,
 }
@@ -158,23 +158,42 @@ def _device_matrix(torch, lib, p, n, seed, mid, kind=0):
     return t
 
 
+def _full_lines(n, lines, seed):
+    """Entry indices of `lines`/2 full rows and `lines`/2 full columns of an
+    n x n matrix (seeded choice)."""
+    rng = np.random.default_rng(seed)
+    r_sel = rng.choice(n, lines // 2, replace=False)
+    c_sel = rng.choice(n, lines // 2, replace=False)
+    rows = np.concatenate([np.repeat(r_sel, n), np.tile(np.arange(n), len(c_sel))])
+    cols = np.concatenate([np.tile(np.arange(n), len(r_sel)), np.repeat(c_sel, n)])
+    return rows, cols
+
+
 @pytest.mark.parametrize("kind", [orc.UNIFORM, orc.WIDE], ids=["uniform", "wide"])
 def test_precision_study_8192(lib, kind):
     """Config-3 study: m = n = k = 8192, uniform and wide draws; normwise and
-    max elementwise error of every form against double-double values of 1024
-    sampled entries of alpha*A*B + beta*C (alpha 1, beta 0.5)."""
+    max elementwise error of every form against double-double values of
+    128 full rows and 128 full columns of alpha*A*B + beta*C (alpha 1,
+    beta 0.5).  The normwise figure is the sampled Frobenius norm scaled to
+    the whole matrix."""
     torch = pytest.importorskip("torch")
-    n, ns = 8192, 1024
-    rng = np.random.default_rng(7)
-    rows, cols = rng.integers(0, n, ns), rng.integers(0, n, ns)
+    n = 8192
+    rows, cols = _full_lines(n, 256, 7)
+    ns = len(rows)
     table = {}
-    for p, forms in (("s", ["plain", "bf16x3", "bf16x6", "ozaki2"]), ("d", ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
+    for p, forms in (("s", ["plain", "bf16x3", "bf16x6", "ozaki2"]),
+                     ("d", ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
         a, b, c0 = (_device_matrix(torch, lib, p, n, 0, i, kind) for i in range(3))
-        ah, bh, ch = (np.asfortranarray(x.cpu().numpy().T) for x in (a, b, c0))
-        hi, lo = orc.dd_gemm_entries(ah, bh, rows, cols, alpha=1.0, beta=0.5, c0=ch)
+        # torch holds the column-major matrices transposed: a.cpu() is A^T in
+        # row-major order, i.e. a column-major A^T, so op(A) = (A^T)^T reads
+        # both operands contiguously in the double-double oracle.
+        at = np.asfortranarray(a.cpu().numpy())
+        bh, ch = (np.asfortranarray(x.cpu().numpy().T) for x in (b, c0))
+        hi, lo = orc.dd_gemm_entries(at, bh, rows, cols, alpha=1.0, beta=0.5, c0=ch, ta=True)
         exact = hi + lo
-        den = (np.linalg.norm(ah.astype(np.float64)) * np.linalg.norm(bh.astype(np.float64)) +
+        den = (np.linalg.norm(at.astype(np.float64)) * np.linalg.norm(bh.astype(np.float64)) +
                0.5 * np.linalg.norm(ch.astype(np.float64)))
+        del at, bh, ch
         fn = getattr(lib, f"mublis_{p}gemm")
         for form in forms:
             assert lib.mublis_b200_set_form(p.encode(), form.encode()) == 0
@@ -190,12 +209,47 @@ def test_precision_study_8192(lib, kind):
         lib.mublis_b200_set_form(p.encode(), b"plain")
         del a, b, c0
         torch.cuda.empty_cache()
-    print(f"\nm=n=k=8192, draw={'wide' if kind else 'uniform'}: normwise, max elementwise rel")
+    print(f"\nm=n=k=8192, draw={'wide' if kind else 'uniform'}, 128 full rows + 128 full "
+          "columns: normwise, max elementwise rel")
     for key, (nw, mx) in table.items():
-        print(f"  {key:14s} {nw:.3e}  {mx:.3e}")
+        print(f"  {key:16s} {nw:.3e}  {mx:.3e}")
     assert table["sgemm bf16x6"][0] <= 1.5 * table["sgemm plain"][0]
     assert table["dgemm ozaki:8"][0] <= table["dgemm plain"][0]
     assert table["dgemm ozaki2"][0] <= table["dgemm plain"][0]
     assert table["sgemm ozaki2"][0] <= table["sgemm plain"][0]
     assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
     assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)
+
+
+def test_dtrsm_8192_forms(lib):
+    """Config-3 DTRSM: n = 8192 with 8192 right-hand sides (left, lower,
+    non-unit, A well conditioned), plain against the emulated off-diagonal
+    updates (the diagonal blocks stay FP64).  16 seeded columns of X are
+    checked against the long-double oracle solve of the same columns."""
+    torch = pytest.importorskip("torch")
+    n, ncheck = 8192, 16
+    a = orc.trsm_matrix(n, np.float64, 3, 0)
+    b = orc.fill(n, n, np.float64, 3, 1)
+    sel = np.sort(np.random.default_rng(11).choice(n, ncheck, replace=False))
+    ref = np.asfortranarray(b[:, sel])
+    orc.set_threads(16)
+    assert orc.restated().oracle_dtrsm(0, 1, 0, 0, n, ncheck, 1.0, a.ctypes.data, 1, n,
+                                       ref.ctypes.data, 1, n) == 0
+    ad = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    b0 = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    errs = {}
+    for form in ("plain", "ozaki2"):
+        assert lib.mublis_b200_set_form(b"d", form.encode()) == 0
+        x = b0.clone()
+        assert lib.mublis_dtrsm(0, 1, 0, 0, n, n, 1.0, ad.data_ptr(), 1, n, x.data_ptr(), 1,
+                                n) == 0, mb.last_error(lib)
+        got = x.cpu().numpy().T[:, sel]
+        d = got - ref
+        errs[form] = (np.linalg.norm(d) / np.linalg.norm(ref),
+                      float(np.max(np.abs(d) / np.maximum(np.abs(ref), 1e-300))))
+    lib.mublis_b200_set_form(b"d", b"plain")
+    print(f"\nDTRSM n=8192, 8192 RHS, {ncheck} columns checked: normwise, max elementwise rel")
+    for form, (nw, mx) in errs.items():
+        print(f"  dtrsm {form:8s} {nw:.3e}  {mx:.3e}")
+    assert errs["plain"][0] <= 4 * n * 2.0 ** -53
+    assert errs["ozaki2"][0] <= 4 * n * 2.0 ** -53
