@@ -785,9 +785,17 @@ __global__ void __launch_bounds__(384, 1)
           for (int j = 0; j < 8; ++j) s0[j] = s1[j] = s2[j] = 0.0;
           const uint2 *base = (const uint2 *)((const uint4 *)R + (size_t)(ch8 >> 1) * C::BM + row) +
                               (ch8 & 1);
-#pragma unroll 1
-          for (int l = 0; l < S; ++l) {
-            const uint2 v = base[(size_t)l * (C::BM * C::BN / 8)];
+          // All residue loads of the chunk first (independent, one round
+          // trip), then the arithmetic: a load-use chain per modulus would
+          // serialise N L2/HBM latencies per chunk.
+          uint2 rv[B200_MAX_MODULI];
+#pragma unroll
+          for (int l = 0; l < B200_MAX_MODULI; ++l)
+            rv[l] = l < S ? base[(size_t)l * (C::BM * C::BN / 8)] : make_uint2(0, 0);
+#pragma unroll
+          for (int l = 0; l < B200_MAX_MODULI; ++l) {
+            if (l >= S) break;
+            const uint2 v = rv[l];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
               const double rr = (double)(int8_t)((j < 4 ? v.x : v.y) >> (8 * (j & 3)));
