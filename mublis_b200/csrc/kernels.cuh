@@ -54,12 +54,13 @@ enum PackXform {
 
 // Pairwise coprime moduli (<= 256) of the modular (CRT) Ozaki form and the
 // constants that reduce an integer modulo each of them without division:
-// c16/c32/c48 = 2^16/2^32/2^48 mod m, magic = floor(2^32 / m) + 1.
+// c19/c38 = 2^19/2^38 mod m; mg = ceil(2^39 / m); bias = floor(m/2) + K m
+// with K m >= 2^29 (see b200_sym_mod).
 constexpr int B200_MAX_MODULI = 16;
 struct B200Moduli {
   int n;
-  int m[B200_MAX_MODULI], c16[B200_MAX_MODULI], c32[B200_MAX_MODULI],
-      c48[B200_MAX_MODULI], magic[B200_MAX_MODULI];
+  int m[B200_MAX_MODULI], c19[B200_MAX_MODULI], c38[B200_MAX_MODULI], bias[B200_MAX_MODULI];
+  unsigned mg[B200_MAX_MODULI];
 };
 
 struct PackOut {
@@ -72,21 +73,18 @@ struct PackOut {
   B200Moduli mod;                    // PACK_INT8_MODULI
 };
 
-// Symmetric residue of t modulo m in [-128, 127] (m <= 256, any int32 t).
-// With magic = floor(2^32/m) + 1 = 2^32/m + d, 0 < d <= 1, mulhi(t, magic)
-// = floor(t/m + e) with |e| = |t| d / 2^32 < 1/2, so it is floor(t/m) up to
-// +-1; r = t - q m lies in [-m, 2m) and two conditional corrections bring it
-// to [0, m) before it is centred.
-__device__ __forceinline__ int b200_sym_mod(int t, int m, int magic) {
-  int r = t - __mulhi(t, magic) * m;
-  r += r < 0 ? m : 0;
-  r -= r >= m ? m : 0;
-  return r > 127 ? r - m : r;
+// Symmetric residue of t modulo m, in [-floor(m/2), m - 1 - floor(m/2)]
+// (within [-128, 127] for m <= 256), for |t| <= 2^29.  u = t + bias lies in
+// [0, 2^31); for u < 2^31 and m <= 2^8, floor(u / m) = umulhi(u, mg) >> 7
+// with mg = ceil(2^39 / m) exactly (Granlund and Montgomery 1994: the error
+// u (mg m - 2^39) / (m 2^39) stays below 1/m; for m = 256 mg is exact), so
+// r = u - q m - floor(m/2) needs no correction.
+__device__ __forceinline__ int b200_sym_mod(int t, int m, unsigned mg, int bias) {
+  const unsigned u = (unsigned)(t + bias);
+  const unsigned q = __umulhi(u, mg) >> 7;
+  return (int)(u - q * (unsigned)m) - (m >> 1);
 }
 
-// Bits of max |x| over kk for every mn of a logical operand view (the
-// Ozaki split's per-row / per-column scale), atomically max-merged into
-// absmax[mn] (which must start at 0).
 template <typename T>
 int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
                   unsigned long long *absmax, cudaStream_t s);

@@ -104,20 +104,20 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
       }
     } else if (o.xform == PACK_INT8_MODULI) {
       // X = rint(x * 2^(bits - e)) is an integer with |X| <= 2^bits <= 2^56,
-      // exact in FP64.  Cut it into 16-bit pieces X = hh 2^48 + hl 2^32 +
-      // lh 2^16 + ll (every step exact), so that X mod m is the residue of
-      // hh c48 + hl c32 + lh c16 + ll, an int32 below 2^26 in magnitude.
+      // exact in FP64.  Cut it into 19-bit pieces X = x2 2^38 + x1 2^19 + x0
+      // (every step exact), so that X mod m is the residue of
+      // x2 c38 + x1 c19 + x0, an int32 below 2^28 in magnitude.
       int8_t *out = (int8_t *)o.out;
       const double x = rint(ldexp((double)val, o.bits - b200_scale_exp(o.absmax[mn])));
-      const double hh = floor(x * 0x1p-48), x1 = fma(-hh, 0x1p48, x);
-      const double hl = floor(x1 * 0x1p-32), x2 = fma(-hl, 0x1p32, x1);
-      const double lh = floor(x2 * 0x1p-16), ll = fma(-lh, 0x1p16, x2);
-      const int ihh = (int)hh, ihl = (int)hl, ilh = (int)lh, ill = (int)ll;
+      const double d2 = floor(x * 0x1p-38), r2 = fma(-d2, 0x1p38, x);
+      const double d1 = floor(r2 * 0x1p-19);
+      const int x2 = (int)d2, x1 = (int)d1, x0 = (int)fma(-d1, 0x1p19, r2);
 #pragma unroll
       for (int t = 0; t < B200_MAX_MODULI; ++t) {  // constant indices: no local copy
         if (t >= o.terms) break;
-        const int v = ihh * o.mod.c48[t] + ihl * o.mod.c32[t] + ilh * o.mod.c16[t] + ill;
-        out[off + t * o.plane_stride] = (int8_t)b200_sym_mod(v, o.mod.m[t], o.mod.magic[t]);
+        const int v = x2 * o.mod.c38[t] + x1 * o.mod.c19[t] + x0;
+        out[off + t * o.plane_stride] =
+            (int8_t)b200_sym_mod(v, o.mod.m[t], o.mod.mg[t], o.mod.bias[t]);
       }
     } else {
       __nv_bfloat16 *out = (__nv_bfloat16 *)o.out;
@@ -163,14 +163,13 @@ __device__ __forceinline__ void kmajor_store8(const PackOut &o, long mn, long of
   } else if (o.xform == PACK_INT8_MODULI) {
     int8_t *out = (int8_t *)o.out;
     const int sh = o.bits - b200_scale_exp(o.absmax[mn]);
-    int hh[8], hl[8], lh[8], ll[8];
+    int x2[8], x1[8], x0[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const double x = rint(ldexp((double)v[j], sh));
-      const double dh = floor(x * 0x1p-48), x1 = fma(-dh, 0x1p48, x);
-      const double dl = floor(x1 * 0x1p-32), x2 = fma(-dl, 0x1p32, x1);
-      const double d3 = floor(x2 * 0x1p-16);
-      hh[j] = (int)dh, hl[j] = (int)dl, lh[j] = (int)d3, ll[j] = (int)fma(-d3, 0x1p16, x2);
+      const double d2 = floor(x * 0x1p-38), r2 = fma(-d2, 0x1p38, x);
+      const double d1 = floor(r2 * 0x1p-19);
+      x2[j] = (int)d2, x1[j] = (int)d1, x0[j] = (int)fma(-d1, 0x1p19, r2);
     }
 #pragma unroll
     for (int t = 0; t < B200_MAX_MODULI; ++t) {
@@ -178,9 +177,8 @@ __device__ __forceinline__ void kmajor_store8(const PackOut &o, long mn, long of
       uint32_t w[2] = {0, 0};
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const int r = b200_sym_mod(hh[j] * o.mod.c48[t] + hl[j] * o.mod.c32[t] +
-                                       lh[j] * o.mod.c16[t] + ll[j],
-                                   o.mod.m[t], o.mod.magic[t]);
+        const int r = b200_sym_mod(x2[j] * o.mod.c38[t] + x1[j] * o.mod.c19[t] + x0[j],
+                                   o.mod.m[t], o.mod.mg[t], o.mod.bias[t]);
         w[j >> 2] |= (uint32_t)(r & 0xff) << (8 * (j & 3));
       }
       *reinterpret_cast<uint2 *>(out + off + t * o.plane_stride) = make_uint2(w[0], w[1]);

@@ -459,7 +459,7 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
 // integer product C' = A'B' is then fixed by its residues modulo every m_l.
 // Each residue plane A'_l = A' mod m_l (int8, symmetric) is packed once, and
 // one int8 GEMM per modulus gives C'_l = A'_l B'_l exactly in int32 (k in
-// chunks of 65536 keeps |C'_l| < 2^30).  The epilogue reduces C'_l mod m_l
+// chunks of 32768 keeps |C'_l| <= 2^29).  The epilogue reduces C'_l mod m_l
 // into a byte per element of a per-CTA residue workspace; after the tile's
 // last modulus it reconstructs C' by the Chinese remainder theorem,
 // C' = sum_l r_l W_l - q M with W_l = (M/m_l) ((M/m_l)^-1 mod m_l) and
@@ -480,14 +480,15 @@ namespace {
 
 constexpr int OZ_MAX_SLICES = 12;
 constexpr int OZ_KCHUNK = 8192;    // k per exact int32 chunk, slice form
-constexpr int OZ2_KCHUNK = 65536;  // k per exact int32 chunk, moduli (|C'_l| <= 2^30)
+constexpr int OZ2_KCHUNK = 32768;  // k per exact int32 chunk, moduli (|C'_l| <= 2^29)
 
 // CRT reconstruction constants of the modular form (host-computed).
 struct OzCrt {
   double w[B200_MAX_MODULI][3];  // W_l cut into 42-bit levels at bits 84 / 42 / 0
   double mlev[3];                // M cut the same way
   double inv_m;                  // 1 / M
-  int m[B200_MAX_MODULI], magic[B200_MAX_MODULI];
+  int m[B200_MAX_MODULI], bias[B200_MAX_MODULI];
+  unsigned mg[B200_MAX_MODULI];
   int bits;                      // pa + pb
 };
 
@@ -717,7 +718,8 @@ __global__ void __launch_bounds__(384, 1)
           tc::tc_fence_after();
           const bool last = ph == nph - 1;
           if constexpr (MOD) {
-            const int m = p.crt.m[pl], magic = p.crt.magic[pl];
+            const int m = p.crt.m[pl], bias = p.crt.bias[pl];
+            const unsigned mg = p.crt.mg[pl];
             uint4 *Rl = (uint4 *)(R + (size_t)pl * C::BM * C::BN) + row;
             // The next chunk's TMEM load is in flight while this one is reduced.
             uint32_t rb[2][16];
@@ -731,10 +733,10 @@ __global__ void __launch_bounds__(384, 1)
               uint32_t out[4] = {0, 0, 0, 0};
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
-                int res = b200_sym_mod((int)rb[ch & 1][j], m, magic);  // |C'_l| <= 2^30
+                int res = b200_sym_mod((int)rb[ch & 1][j], m, mg, bias);  // |C'_l| <= 2^29
                 if (cc > 0) {
                   const uint32_t word = j < 4 ? prev.x : j < 8 ? prev.y : j < 12 ? prev.z : prev.w;
-                  res = b200_sym_mod(res + (int)(int8_t)(word >> (8 * (j & 3))), m, magic);
+                  res = b200_sym_mod(res + (int)(int8_t)(word >> (8 * (j & 3))), m, mg, bias);
                 }
                 out[j >> 2] |= (uint32_t)(res & 0xff) << (8 * (j & 3));
               }
@@ -858,10 +860,10 @@ int oz2_setup(int N, long k, int pmax, B200Moduli *mod, OzCrt *crt, int *pa, int
   for (int l = 0; l < N; ++l) {
     const int m = OZ2_MODULI[l];
     mod->m[l] = crt->m[l] = m;
-    mod->c16[l] = (int)((1u << 16) % (unsigned)m);
-    mod->c32[l] = (int)((((u128)1) << 32) % (u128)m);
-    mod->c48[l] = (int)((((u128)1) << 48) % (u128)m);
-    mod->magic[l] = crt->magic[l] = (int)((1ull << 32) / (unsigned long long)m + 1);
+    mod->c19[l] = (int)((1u << 19) % (unsigned)m);
+    mod->c38[l] = (int)((((u128)1) << 38) % (u128)m);
+    mod->mg[l] = crt->mg[l] = (unsigned)(((1ull << 39) + (unsigned long long)m - 1) / m);
+    mod->bias[l] = crt->bias[l] = m / 2 + (int)(((1u << 29) + m - 1) / m) * m;
     const u128 Ml = M / (u128)m;
     const int r = (int)(Ml % (u128)m);
     int y = 1;

@@ -130,7 +130,7 @@ def test_wide_range_inputs_ozaki(lib):
 @pytest.mark.parametrize("form", ["ozaki:8", "ozaki2"])
 def test_ozaki_long_k_chunks(lib, form):
     """k = 70001 spans several exact-int32 chunks of both integer forms
-    (8192 for slices, 65536 for moduli): the per-chunk partial results must
+    (8192 for slices, 32768 for moduli): the per-chunk partial results must
     combine to the double-double value of sampled entries."""
     m, n, k = 200, 136, 70001
     a = orc.fill(m, k, np.float64, 9, 0)
