@@ -103,6 +103,22 @@ int mublis_b200_plan_trsm_grouped(char dtype, const mublis_b200_trsm_problem_t *
 int mublis_b200_plan_run(mublis_b200_plan_t *plan);
 int mublis_b200_plan_destroy(mublis_b200_plan_t *plan);
 
+/* Tuned-tile table (the replacement for the reference's compile-time block
+ * sizes, targets/<t>/context.c, which a B200 build finds by timing instead).
+ * The autotuner's choices (per precision, size class and problem-count
+ * bucket) can be kept on disk.  A file is keyed by the GPU (name, SM count,
+ * compute capability) and the driver version: loading a file written on
+ * another GPU or driver loads nothing.  If MUBLIS_B200_TUNE_FILE names a
+ * file, the library loads it at initialisation and rewrites it whenever the
+ * autotuner adds a choice.
+ *   save:  write the current table to `path` (atomically: temp + rename);
+ *   load:  merge `path` into the table, *entries = choices loaded (0 when
+ *          the file is missing or keyed to another GPU / driver);
+ *   reset: forget every choice (the defaults apply until re-tuned). */
+int mublis_b200_tune_save(const char *path);
+int mublis_b200_tune_load(const char *path, int *entries);
+int mublis_b200_tune_reset(void);
+
 /* ---- request server (no counterpart in the reference) -------------------
  * Continuous batching of Level-3 calls issued by many host threads.  Once a
  * server is attached, every cblas_* / mublis_* call whose operands are ALL

@@ -136,6 +136,9 @@ EXTENSIONS = {
     "mublis_b200_server_free": ([_P, _P], _I),
     "mublis_b200_server_stats": ([_P, ctypes.POINTER(ServerStats)], _I),
     "mublis_b200_server_reset_stats": ([_P], _I),
+    "mublis_b200_tune_save": ([ctypes.c_char_p], _I),
+    "mublis_b200_tune_load": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)], _I),
+    "mublis_b200_tune_reset": ([], _I),
     "mublis_b200_sgemm_noalloc": ([_I, _I, _I, _I, _I, ctypes.c_float, _P, _I, _I, _P, _I, _I,
                                    ctypes.c_float, _P, _I, _I], _I),
 }

@@ -45,6 +45,10 @@ enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM
  * given (slices may be NULL). */
 int b200_parse_form(const char *s, int *slices);
 
+/* Loads the tuned-tile table named by MUBLIS_B200_TUNE_FILE, if any (called
+ * once at initialisation). */
+void b200_tune_autoload(void);
+
 /* One product C(ji) := alpha * sum_t A_t B_t + beta * C over the domain of
  * `product`.  npairs is 1, or 2 for SYR2K (both pairs share the product's
  * operand structure and are concatenated along k). */
@@ -98,6 +102,33 @@ int b200_get_default_slices(int dtype);
 /* Strided copies between caller host memory and a compact device buffer of
  * rows x cols with leading dimension ld (column-major).  The host side may
  * have any (rs, cs). */
+/* Column-panel pipeline for host-resident operands.  The output (and an
+ * optional input with the same columns) are moved in panels of columns:
+ * panel J's host->device copy, its computation and panel J-1's copy back run
+ * on three streams at once (PCIe is full duplex), so the transfers of a
+ * large call overlap its own arithmetic.  `run` computes one panel on the
+ * calling thread's library stream.  A view can be moved by panels when one
+ * of its strides is 1 (b200_colpipe_view_ok). */
+typedef struct {
+  const void *host; /* NULL: no such operand */
+  long rows, rs, cs;
+} b200_colpipe_view_t;
+typedef struct {
+  size_t elt;
+  long ncols;
+  b200_colpipe_view_t in;  /* read-only input panel (op(B)), or host NULL */
+  b200_colpipe_view_t out; /* output panel (C, or B in place) */
+  int out_read;            /* copy the output panel in before computing */
+  int (*run)(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
+             void *out_dev, long out_rs, long out_cs);
+  void *ctx;
+} b200_colpipe_t;
+int b200_colpipe_view_ok(long rows, long rs, long cs);
+/* Number of panels worth using for ncols columns of total bytes (< 2: do
+ * not pipeline). */
+int b200_colpipe_panels(long ncols, size_t bytes);
+int b200_column_pipeline(const b200_colpipe_t *p);
+
 int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long rows, long cols,
                   size_t elt);
 int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,

@@ -43,9 +43,18 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// Tile idx -> (tm, tn), rasterised in groups of 8 along M so that CTAs
-// running together share B strips in L2.
+// Tile idx -> (tm, tn): from the host's tile list when the domain
+// restricts the output or the k-ranges (only the tiles that write, heaviest
+// first, so the strided assignment to persistent CTAs stays balanced), else
+// rasterised in groups of 8 along M so that CTAs running together share B
+// strips in L2.
 __device__ __forceinline__ void tile_coords(const DmmaGemmArgs &p, int idx, int &tm, int &tn) {
+  if (p.tile_list) {
+    const int2 t = p.tile_list[idx];
+    tm = t.x;
+    tn = t.y;
+    return;
+  }
   constexpr int G = 8;
   const int group = idx / (G * p.tiles_n);
   const int first_m = group * G;
@@ -89,7 +98,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc::fence_barrier_init();
   }
   __syncthreads();
-  const int num_tiles = p.tiles_m * p.tiles_n;
+  const int num_tiles = p.tile_list ? p.ntiles : p.tiles_m * p.tiles_n;
 
   if (warp == CONSUMERS) {
     // ---------------- producer ----------------
@@ -190,7 +199,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 }  // namespace
 
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s) {
-  const long tiles = (long)a.tiles_m * a.tiles_n;
+  const long tiles = a.tile_list ? a.ntiles : (long)a.tiles_m * a.tiles_n;
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "dgemm: too many tiles");
   static bool configured = false;

@@ -19,6 +19,7 @@
 // (:111-112, :224-225).  A tile with an empty k-range writes beta*C, which is
 // the reference's "no update" pass (:88-121).
 #include <cstdlib>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -44,7 +45,8 @@ __device__ __forceinline__ void lds16(double (&d)[2], const double *p) {
   d[0] = v.x; d[1] = v.y;
 }
 
-template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB>
+template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB,
+          bool PAIR = false>
 __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p) {
   constexpr int NT = 256;
   constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;
@@ -90,11 +92,21 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
   const int wm = warp % WARPS_M, wn = warp / WARPS_M;
   const int ty = lane >> 3, tx = lane & 7;
 
-  T acc[TM][TN];
+  // PAIR (FP32 only): accumulators as column pairs updated with the packed
+  // sm_100 FMA (__ffma2_rn: two correctly rounded fmaf per instruction), so
+  // the FMA stream takes half the issue slots and the loads and address
+  // arithmetic fit beside it.  Each element's result is that of fmaf.
+  static_assert(!PAIR || (sizeof(T) == 4 && TN % 2 == 0), "pairs are FP32 column pairs");
+  constexpr int TNP = PAIR ? TN / 2 : TN;
+  using Acc = typename std::conditional<PAIR, float2, T>::type;
+  Acc acc[TM][TNP];
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+    for (int j = 0; j < TNP; ++j) {
+      if constexpr (PAIR) acc[i][j] = make_float2(0.f, 0.f);
+      else acc[i][j] = T(0);
+    }
 
   auto load_stage = [&](int stage, int kt) {
     const T *ga = p.ap + (long)kt * BK * p.lda + m0;
@@ -149,7 +161,13 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+        for (int j = 0; j < TNP; ++j) {
+          if constexpr (PAIR)
+            acc[i][j] = __ffma2_rn(make_float2(af[i], af[i]), make_float2(bf[2 * j], bf[2 * j + 1]),
+                                   acc[i][j]);
+          else
+            acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+        }
     }
   }
   cp_async_wait<0>();
@@ -164,7 +182,9 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
       const long gj = n0 + wn * WTN + (j / CW) * NSP + tx * CW + (j % CW);
       if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
       T *cij = p.c + gi * p.rs_c + gj * p.cs_c;
-      T v = alpha * acc[i][j];
+      T v;
+      if constexpr (PAIR) v = alpha * ((j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x);
+      else v = alpha * acc[i][j];
       if (beta != T(0)) v = fma(beta, *cij, v);
       *cij = v;
     }
@@ -188,10 +208,10 @@ __global__ void scale_kernel(int m, int n, T beta, T *c, long rs, long cs, int j
 // stages, min CTAs per SM).  Packed panels are padded to 128 in M and N, so
 // every configuration reads the same panels.  Index 0 is the default; the
 // others are kept for tuning (MUBLIS_B200_SIMT_S / MUBLIS_B200_SIMT_D).
-template <typename T, int BM, int BN, int WM, int WN, int ST, int MINB>
+template <typename T, int BM, int BN, int WM, int WN, int ST, int MINB, bool PAIR = false>
 int launch_cfg(const SimtGemmArgs<T> &a, cudaStream_t s) {
   constexpr int BK = SimtConfig<T>::BK;
-  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB>;
+  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR>;
   const size_t smem = (size_t)ST * BK * (BM + BN) * sizeof(T);
   static bool configured = false;
   if (!configured) {
@@ -226,6 +246,7 @@ int launch_simt_gemm<float>(const SimtGemmArgs<float> &a, cudaStream_t s) {
   switch (simt_variant(false)) {
   case 1: return launch_cfg<float, 128, 128, 2, 4, 4, 2>(a, s);
   case 2: return launch_cfg<float, 128, 128, 4, 2, 3, 1>(a, s);
+  case 3: return launch_cfg<float, 128, 128, 4, 2, 4, 2, true>(a, s);
   default: return launch_cfg<float, 128, 128, 4, 2, 4, 2>(a, s);
   }
 }

@@ -12,7 +12,10 @@
 // on one CTA.
 #include <algorithm>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -361,6 +364,95 @@ int run_groups(GemmGroup (&g)[NCLASS], cudaStream_t s) {
 std::mutex g_tune_mu;
 int g_tuned[2][NCLASS][32];  // 0 = untuned, else variant + 1
 
+// ---- tuned-table persistence ---------------------------------------------
+//
+// Text file: one key line, then one line per choice,
+//   mublis_b200-tune <gpu name> sms=<n> cc=<major>.<minor> driver=<v> table=1
+//   gemm <fp64 0/1> <size class> <count bucket> <tile variant>
+// The key ties the file to a GPU model and driver (tile timings change with
+// either); table=1 names this library's classes and variants.
+
+constexpr int kTuneTable = 1;
+
+std::string tune_key() {
+  int dev = 0, drv = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return std::string();
+  cudaDriverGetVersion(&drv);
+  std::string name(prop.name);
+  for (char &ch : name)
+    if (ch == ' ' || ch == '\t') ch = '_';
+  char buf[512];
+  snprintf(buf, sizeof buf, "mublis_b200-tune %s sms=%d cc=%d.%d driver=%d table=%d",
+           name.c_str(), prop.multiProcessorCount, prop.major, prop.minor, drv, kTuneTable);
+  return buf;
+}
+
+int tune_save(const char *path) {
+  if (!path || !*path) return b200_set_error(B200_EINVAL, "tune: empty path");
+  const std::string key = tune_key();
+  if (key.empty()) return b200_set_error(B200_ECUDA, "tune: no device to key the table to");
+  std::string text = key + "\n";
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int dt = 0; dt < 2; ++dt)
+      for (int c = 0; c < NCLASS; ++c)
+        for (int b = 0; b < 32; ++b)
+          if (g_tuned[dt][c][b]) {
+            char line[64];
+            snprintf(line, sizeof line, "gemm %d %d %d %d\n", dt, c, b, g_tuned[dt][c][b] - 1);
+            text += line;
+          }
+  }
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE *f = fopen(tmp.c_str(), "w");
+  if (!f) return b200_set_error(B200_EINVAL, "tune: cannot write the table file");
+  const bool ok = fwrite(text.data(), 1, text.size(), f) == text.size();
+  if (fclose(f) != 0 || !ok || rename(tmp.c_str(), path) != 0) {
+    remove(tmp.c_str());
+    return b200_set_error(B200_EINVAL, "tune: cannot write the table file");
+  }
+  return B200_OK;
+}
+
+int tune_load(const char *path, int *entries) {
+  if (entries) *entries = 0;
+  if (!path || !*path) return b200_set_error(B200_EINVAL, "tune: empty path");
+  FILE *f = fopen(path, "r");
+  if (!f) return B200_OK;  // no table yet
+  const std::string key = tune_key();
+  char line[512];
+  int loaded = 0;
+  if (!key.empty() && fgets(line, sizeof line, f)) {
+    line[strcspn(line, "\r\n")] = 0;
+    if (key == line) {
+      while (fgets(line, sizeof line, f)) {
+        int dt, c, b, v;
+        if (sscanf(line, "gemm %d %d %d %d", &dt, &c, &b, &v) != 4) continue;
+        if (dt < 0 || dt > 1 || c < 0 || c >= NCLASS || b < 0 || b >= 32 || v < 0 ||
+            v >= TILE_VARIANTS)
+          continue;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[dt][c][b] = v + 1;
+        ++loaded;
+      }
+    }
+  }
+  fclose(f);
+  if (entries) *entries = loaded;
+  return B200_OK;
+}
+
+const char *tune_env_path() {
+  const char *p = getenv("MUBLIS_B200_TUNE_FILE");
+  return p && *p ? p : nullptr;
+}
+
+void b200_tune_autosave() {
+  if (const char *p = tune_env_path()) tune_save(p);  // best effort: tuning goes on regardless
+}
+
 template <typename T>
 int autotune(std::vector<GemmEntry> (&cls)[NCLASS], GemmGroup (&g)[NCLASS], cudaStream_t s) {
   const int dt = sizeof(T) == 8;
@@ -394,8 +486,11 @@ int autotune(std::vector<GemmEntry> (&cls)[NCLASS], GemmGroup (&g)[NCLASS], cuda
       if (ms_best < best) { best = ms_best; best_v = v; }
     }
     B200_TRY(build_group(cls[c], best_v, g[c], s));
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[dt][c][bucket] = best_v + 1;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tuned[dt][c][bucket] = best_v + 1;
+    }
+    b200_tune_autosave();
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -794,3 +889,26 @@ int mublis_b200_plan_destroy(mublis_b200_plan_t *plan) {
 }
 
 }  // extern "C"
+
+// ---- tuned-table API (include/mublis_b200.h) ---------------------------------
+
+extern "C" void b200_tune_autoload(void) {
+  if (const char *p = tune_env_path()) tune_load(p, nullptr);
+}
+
+extern "C" int mublis_b200_tune_save(const char *path) {
+  B200_TRY(b200_init());
+  return tune_save(path);
+}
+
+extern "C" int mublis_b200_tune_load(const char *path, int *entries) {
+  if (entries) *entries = 0;
+  B200_TRY(b200_init());
+  return tune_load(path, entries);
+}
+
+extern "C" int mublis_b200_tune_reset(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  memset(g_tuned, 0, sizeof g_tuned);
+  return B200_OK;
+}

@@ -94,11 +94,87 @@ int b200_stage_end(b200_stage_set_t *ss, int status) {
 
 static size_t elt_of(int dtype) { return dtype == B200_F64 ? sizeof(double) : sizeof(float); }
 
+/* ---- column-panel pipelining of host operands ----------------------------
+ *
+ * A large call whose output columns are independent (no triangle restriction
+ * on C, a plain op(B) whose columns feed only the same columns of C, or a
+ * left TRSM / TRMM whose right-hand sides are independent) moves its output
+ * and op(B) through the device in panels of columns, overlapping each
+ * panel's transfers with the arithmetic of its neighbours
+ * (b200_column_pipeline).  A is staged whole first. */
+
+static int pipelinable(const void *p, long rows, long rs, long cs) {
+  return p != NULL && !b200_is_device_ptr(p) && b200_colpipe_view_ok(rows, rs, cs);
+}
+
+static int l3_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
+                    void *out_dev, long out_rs, long out_cs) {
+  (void)j0;
+  b200_l3_desc_t d = *(const b200_l3_desc_t *)ctx;
+  d.n = (int)cols;
+  d.b[0] = in_dev ? in_dev : out_dev; /* in place when there is no separate input */
+  d.rs_b[0] = in_dev ? in_rs : out_rs;
+  d.cs_b[0] = in_dev ? in_cs : out_cs;
+  d.c = out_dev;
+  d.rs_c = out_rs;
+  d.cs_c = out_cs;
+  return b200_l3_run(&d);
+}
+
+static int trsm_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
+                      void *out_dev, long out_rs, long out_cs) {
+  (void)j0, (void)in_dev, (void)in_rs, (void)in_cs;
+  b200_trsm_desc_t d = *(const b200_trsm_desc_t *)ctx;
+  d.n = (int)cols;
+  d.b = out_dev;
+  d.rs_b = out_rs;
+  d.cs_b = out_cs;
+  return b200_trsm_run(&d);
+}
+
+/* The l3 call as a pipeline over the columns of C, or 0 when it does not
+ * qualify (the caller then stages everything at once). */
+static int try_pipeline_l3(const b200_l3_desc_t *d, int *status) {
+  if (b200_serve_attached() || d->npairs != 1 || d->alpha == 0.0 || d->k <= 0) return 0;
+  const mublis_l3_product_t *pr = &d->product;
+  if (pr->domain.ji != MUBLIS_L3_ALL || pr->domain.jp != MUBLIS_L3_ALL ||
+      pr->b.struc != MUBLIS_STRUC_GENERAL || d->b[0] == d->c)
+    return 0;
+  if (!pipelinable(d->b[0], d->k, d->rs_b[0], d->cs_b[0]) ||
+      !pipelinable(d->c, d->m, d->rs_c, d->cs_c))
+    return 0;
+  const size_t elt = elt_of(d->dtype);
+  if (b200_colpipe_panels(d->n, (size_t)(d->k + d->m) * d->n * elt) < 2) return 0;
+  b200_stage_set_t ss;
+  b200_stage_begin(&ss, elt);
+  b200_l3_desc_t dd = *d;
+  b200_view_t v;
+  int st = b200_stage_view(&ss, d->a[0], d->m, d->k, d->rs_a[0], d->cs_a[0], 1, 0, &v);
+  dd.a[0] = v.ptr;
+  dd.rs_a[0] = v.rs;
+  dd.cs_a[0] = v.cs;
+  if (st == B200_OK) {
+    b200_colpipe_t p;
+    memset(&p, 0, sizeof p);
+    p.elt = elt;
+    p.ncols = d->n;
+    p.in.host = d->b[0], p.in.rows = d->k, p.in.rs = d->rs_b[0], p.in.cs = d->cs_b[0];
+    p.out.host = d->c, p.out.rows = d->m, p.out.rs = d->rs_c, p.out.cs = d->cs_c;
+    p.out_read = d->beta != 0.0;
+    p.run = l3_panel;
+    p.ctx = &dd;
+    st = b200_column_pipeline(&p);
+  }
+  *status = b200_stage_end(&ss, st);
+  return 1;
+}
+
 int b200_front_l3(b200_l3_desc_t *d) {
   if (d->m == 0 || d->n == 0) return B200_OK;
   if (d->m < 0 || d->n < 0 || d->k < 0) return b200_set_error(B200_EINVAL, "negative size");
   int st = b200_init();
   if (st != B200_OK) return st;
+  if (try_pipeline_l3(d, &st)) return st;
 
   b200_stage_set_t ss;
   b200_stage_begin(&ss, elt_of(d->dtype));
@@ -145,7 +221,16 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   b200_stage_set_t ss;
   b200_stage_begin(&ss, elt_of(dtype));
   b200_view_t vb, va;
-  st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  /* Left side with host B: the right-hand sides are independent, so B goes
+   * through the device in column panels (B stays unstaged here). */
+  const int piped = side == MUBLIS_LEFT && alpha != 0.0 && !b200_serve_attached() &&
+                    pipelinable(b, m, rs_b, cs_b) &&
+                    b200_colpipe_panels(n, (size_t)m * n * elt_of(dtype)) >= 2;
+  if (piped) {
+    vb.ptr = b, vb.rs = rs_b, vb.cs = cs_b;
+  } else {
+    st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  }
   if (st == B200_OK && alpha == 0.0) {
     st = b200_scale_strided(dtype, m, n, 0.0, vb.ptr, vb.rs, vb.cs, MUBLIS_L3_ALL);
     return b200_stage_end(&ss, st);
@@ -196,6 +281,18 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   d.c = vb.ptr;
   d.rs_c = vb.rs;
   d.cs_c = vb.cs;
+  if (piped) {
+    b200_colpipe_t p;
+    memset(&p, 0, sizeof p);
+    p.elt = elt_of(dtype);
+    p.ncols = n;
+    p.out.host = b, p.out.rows = m, p.out.rs = rs_b, p.out.cs = cs_b;
+    p.out_read = 1;
+    p.run = l3_panel;
+    p.ctx = &d;
+    st = b200_column_pipeline(&p);
+    return b200_stage_end(&ss, st);
+  }
   st = ss.n == 0 && b200_serve_attached() ? b200_serve_l3(&d) : b200_l3_run(&d);
   return b200_stage_end(&ss, st);
 }
@@ -210,7 +307,18 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   b200_stage_set_t ss;
   b200_stage_begin(&ss, elt_of(dtype));
   b200_view_t vb, va;
-  st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  /* Host B: the right-hand sides (columns of the normalised left solve) are
+   * independent, so B goes through the device in panels (unstaged here). */
+  const long m_left = side == MUBLIS_LEFT ? m : n, n_left = side == MUBLIS_LEFT ? n : m;
+  const long rs_left = side == MUBLIS_LEFT ? rs_b : cs_b, cs_left = side == MUBLIS_LEFT ? cs_b : rs_b;
+  const int piped = alpha != 0.0 && !b200_serve_attached() &&
+                    pipelinable(b, m_left, rs_left, cs_left) &&
+                    b200_colpipe_panels(n_left, (size_t)m * n * elt_of(dtype)) >= 2;
+  if (piped) {
+    vb.ptr = b, vb.rs = rs_b, vb.cs = cs_b;
+  } else {
+    st = b200_stage_view(&ss, b, m, n, rs_b, cs_b, alpha != 0.0, 1, &vb);
+  }
   if (st == B200_OK && alpha == 0.0) { /* trsm.c:27-33 */
     st = b200_scale_strided(dtype, m, n, 0.0, vb.ptr, vb.rs, vb.cs, MUBLIS_L3_ALL);
     return b200_stage_end(&ss, st);
@@ -244,6 +352,18 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   d.uplo = uplo;
   d.unit_diag = diag == MUBLIS_UNIT_DIAG;
   d.form = B200_FORM_AUTO;
+  if (piped) {
+    b200_colpipe_t p;
+    memset(&p, 0, sizeof p);
+    p.elt = elt_of(dtype);
+    p.ncols = n;
+    p.out.host = b, p.out.rows = m, p.out.rs = brs, p.out.cs = bcs;
+    p.out_read = 1;
+    p.run = trsm_panel;
+    p.ctx = &d;
+    st = b200_column_pipeline(&p);
+    return b200_stage_end(&ss, st);
+  }
   st = ss.n == 0 && b200_serve_attached() ? b200_serve_trsm(&d) : b200_trsm_run(&d);
   return b200_stage_end(&ss, st);
 }

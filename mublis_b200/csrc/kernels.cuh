@@ -122,6 +122,8 @@ struct DmmaGemmArgs {
   long rs_c, cs_c;
   int m, n, k;
   int tiles_m, tiles_n;
+  const int2 *tile_list;  // (tm, tn) of the tiles to compute, or null: all tiles
+  int ntiles;             // entries of tile_list
   double alpha, beta;
   int jp, ji, pi;
   int *err;

@@ -9,7 +9,9 @@
 // once for the whole call (one HBM pass, pack.cu) and the contraction kernel
 // tiles the entire output on the device.
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "kernels.cuh"
 #include "tc_common.cuh"
@@ -21,17 +23,19 @@ namespace {
 // plain kernel's: the tensor-core forms pay a split/residue pass and, for
 // the integer forms, one int8 product per modulus, so below these sizes
 // (crossovers measured on B200) plain wins.  FP32: BF16x6 (3-term split,
-// error equal to plain FP32) when min(m, n) and k are >= 512.  FP64: the
-// modular Ozaki form with 16 moduli (error ~36x below plain FP64) when
-// min(m, n) and k are >= 4096 (at 2048^3 plain is faster, at 4096^3 the
-// modular form is 1.8x plain, at 8192^3 2.9x).
+// error equal to plain FP32) when min(m, n) and k are >= 512 (at 256 x 8192
+// x 256 plain is faster).  FP64: the modular Ozaki form with 16 moduli (error
+// ~36x below plain FP64) when min(m, n) and k are >= 1024 and m n >= 2048^2,
+// i.e. at least 64 of its 256 x 256 tiles (measured: 2048^3 0.65 vs 0.71 ms,
+// 1024 x 8192 x 1024 0.58 vs 0.76, 2048 x 8192 x 2048 1.28 vs 2.26, 8192^3
+// 8.8 vs 32.4; at 1024 x 1024 x 8192 the two tie).
 int resolve_form(const b200_l3_desc_t *d) {
   int f = d->form == B200_FORM_AUTO ? b200_get_default_form(d->dtype) : d->form;
   if (f == B200_FORM_POLICY) {
     const long m = d->m, n = d->n, k = (long)d->k * d->npairs;
     const long mn = m < n ? m : n;
     if (d->dtype == B200_F32) return mn >= 512 && k >= 512 ? B200_FORM_BF16X6 : B200_FORM_PLAIN;
-    return mn >= 4096 && k >= 4096 ? B200_FORM_OZAKI2 : B200_FORM_PLAIN;
+    return mn >= 1024 && k >= 1024 && m * n >= 2048L * 2048 ? B200_FORM_OZAKI2 : B200_FORM_PLAIN;
   }
   if (d->dtype == B200_F32 && f == B200_FORM_OZAKI) f = B200_FORM_PLAIN;
   if (d->dtype == B200_F64 && (f == B200_FORM_BF16X3 || f == B200_FORM_BF16X6)) f = B200_FORM_PLAIN;
@@ -81,7 +85,43 @@ int run_dmma(const b200_l3_desc_t *d) {
     PackOut ob{bp, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
     st = pack_pairs<double>(d, oa, mpad, ob, npad, kpad, s);
   }
-  if (st == B200_OK) {
+  // Restricted domains: list the tiles that write (ji) with their k-range
+  // (jp, pi), heaviest first (the host twin of the kernel's tile_krange).
+  const int tiles_m = (int)(mpad / B200_DMMA_TILE), tiles_n = (int)(npad / B200_DMMA_TILE);
+  const mublis_l3_domain_t &dom = d->product.domain;
+  void *list = nullptr;
+  int ntiles = 0;
+  if (st == B200_OK &&
+      (dom.ji != MUBLIS_L3_ALL || dom.jp != MUBLIS_L3_ALL || dom.pi != MUBLIS_L3_ALL)) {
+    std::vector<std::pair<long, int2>> tl;
+    const long T = B200_DMMA_TILE, BK = B200_DMMA_BK;
+    for (int tm = 0; tm < tiles_m; ++tm)
+      for (int tn = 0; tn < tiles_n; ++tn) {
+        const long m0 = tm * T, n0 = tn * T;
+        if (dom.ji == MUBLIS_L3_LOWER && n0 >= m0 + T) continue;
+        if (dom.ji == MUBLIS_L3_UPPER && n0 + T <= m0) continue;
+        long kb = 0, ke = ktot;
+        if (dom.jp == MUBLIS_L3_LOWER) kb = std::max(kb, n0);
+        if (dom.jp == MUBLIS_L3_UPPER) ke = std::min(ke, n0 + T);
+        if (dom.pi == MUBLIS_L3_LOWER) ke = std::min(ke, m0 + T);
+        if (dom.pi == MUBLIS_L3_UPPER) kb = std::max(kb, m0);
+        const long cost = ke > kb ? (ke + BK - 1) / BK - kb / BK : 0;
+        tl.push_back({cost, make_int2(tm, tn)});
+      }
+    std::stable_sort(tl.begin(), tl.end(),
+                     [](const std::pair<long, int2> &x, const std::pair<long, int2> &y) {
+                       return x.first > y.first;
+                     });
+    std::vector<int2> flat(tl.size());
+    for (size_t i = 0; i < tl.size(); ++i) flat[i] = tl[i].second;
+    ntiles = (int)flat.size();
+    st = b200_alloc(&list, sizeof(int2) * (ntiles > 0 ? ntiles : 1));
+    if (st == B200_OK && ntiles > 0 &&
+        cudaMemcpyAsync(list, flat.data(), sizeof(int2) * ntiles, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess)
+      st = b200_set_error(B200_ECUDA, "dgemm: tile list upload failed");
+  }
+  if (st == B200_OK && (list == nullptr || ntiles > 0)) {
     DmmaGemmArgs g;
     g.ap = (const double *)ap;
     g.bp = (const double *)bp;
@@ -92,8 +132,10 @@ int run_dmma(const b200_l3_desc_t *d) {
     g.m = d->m;
     g.n = d->n;
     g.k = (int)ktot;
-    g.tiles_m = (int)(mpad / B200_DMMA_TILE);
-    g.tiles_n = (int)(npad / B200_DMMA_TILE);
+    g.tiles_m = tiles_m;
+    g.tiles_n = tiles_n;
+    g.tile_list = (const int2 *)list;
+    g.ntiles = ntiles;
     g.alpha = d->alpha;
     g.beta = d->beta;
     g.jp = d->product.domain.jp;
@@ -102,6 +144,7 @@ int run_dmma(const b200_l3_desc_t *d) {
     g.err = b200_device_error_word();
     st = launch_dmma_gemm(g, s);
   }
+  b200_free(list);
   b200_free(ap);
   b200_free(bp);
   return st;

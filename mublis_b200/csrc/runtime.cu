@@ -77,6 +77,7 @@ void do_init() {
   if (slices > 0) g_default_slices[B200_F64] = slices;
   if (sslices > 0) g_default_slices[B200_F32] = sslices;
   g_init_status = B200_OK;
+  b200_tune_autoload();
 }
 
 }  // namespace
@@ -255,6 +256,120 @@ int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long ro
   free(stage);
   B200_CUDA_TRY(e);
   return B200_OK;
+}
+
+// ---- column-panel pipeline (host-resident operands) --------------------------
+
+namespace {
+
+thread_local cudaStream_t t_copy_in = nullptr, t_copy_out = nullptr;
+
+int copy_streams() {
+  if (!t_copy_in) B200_CUDA_TRY(cudaStreamCreateWithFlags(&t_copy_in, cudaStreamNonBlocking));
+  if (!t_copy_out) B200_CUDA_TRY(cudaStreamCreateWithFlags(&t_copy_out, cudaStreamNonBlocking));
+  return B200_OK;
+}
+
+// Panel [j0, j0 + cols) of a host view as a 2-D copy.  rs == 1: columns are
+// contiguous, the device panel is column-major (ld = rows).  cs == 1: rows
+// are contiguous, the device panel is row-major (ld = cols).
+struct PanelCopy {
+  size_t width, height, hpitch, dpitch;
+  long off, drs, dcs;
+};
+
+PanelCopy panel_copy(const b200_colpipe_view_t &v, long j0, long cols, size_t elt) {
+  PanelCopy c;
+  if (v.rs == 1) {
+    c.width = v.rows * elt, c.height = cols, c.hpitch = (cols == 1 ? v.rows : v.cs) * elt;
+    c.dpitch = v.rows * elt, c.off = j0 * v.cs, c.drs = 1, c.dcs = v.rows;
+  } else {
+    c.width = cols * elt, c.height = v.rows, c.hpitch = v.rs * elt;
+    c.dpitch = cols * elt, c.off = j0, c.drs = cols, c.dcs = 1;
+  }
+  return c;
+}
+
+}  // namespace
+
+int b200_colpipe_view_ok(long rows, long rs, long cs) {
+  return rs == 1 ? cs >= rows : (cs == 1 && rs >= 1);
+}
+
+int b200_colpipe_panels(long ncols, size_t bytes) {
+  if (bytes < (32u << 20)) return 1;
+  long p = ncols / 1024;
+  return (int)(p > 4 ? 4 : p);
+}
+
+int b200_column_pipeline(const b200_colpipe_t *p) {
+  B200_TRY(copy_streams());
+  cudaStream_t sc = b200_cur_stream(), si = t_copy_in, so = t_copy_out;
+  const int npan = b200_colpipe_panels(p->ncols, 1ull << 40);
+  const long w = b200_round_up(b200_ceil_div(p->ncols, npan < 1 ? 1 : npan), 128);
+  const bool has_in = p->in.host != nullptr;
+  const size_t in_bytes = has_in ? (size_t)p->in.rows * w * p->elt : 0;
+  const size_t out_bytes = (size_t)p->out.rows * w * p->elt;
+  void *buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2][3] = {};  // per slot: copied in, computed, copied out
+  int st = B200_OK;
+  for (int q = 0; q < 2 && st == B200_OK; ++q) {
+    st = b200_alloc(&buf[q], in_bytes + out_bytes);
+    for (int e = 0; e < 3 && st == B200_OK; ++e)
+      if (cudaEventCreateWithFlags(&ev[q][e], cudaEventDisableTiming) != cudaSuccess)
+        st = b200_set_error(B200_ECUDA, "pipeline: event creation failed");
+  }
+  cudaEvent_t ready = nullptr;
+  if (st == B200_OK && (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess ||
+                        cudaEventRecord(ready, sc) != cudaSuccess ||
+                        cudaStreamWaitEvent(si, ready, 0) != cudaSuccess))
+    st = b200_set_error(B200_ECUDA, "pipeline: stream ordering failed");
+  long issued = 0;
+  for (long j0 = 0; j0 < p->ncols && st == B200_OK; j0 += w, ++issued) {
+    const long cols = p->ncols - j0 < w ? p->ncols - j0 : w;
+    const int q = (int)(issued & 1);
+    char *in_dev = (char *)buf[q], *out_dev = (char *)buf[q] + in_bytes;
+    if (issued >= 2) {  // the slot's previous panel has been computed and copied out
+      cudaStreamWaitEvent(si, ev[q][1], 0);
+      cudaStreamWaitEvent(si, ev[q][2], 0);
+    }
+    const PanelCopy ci = has_in ? panel_copy(p->in, j0, cols, p->elt) : PanelCopy{};
+    const PanelCopy co = panel_copy(p->out, j0, cols, p->elt);
+    cudaError_t e = cudaSuccess;
+    if (has_in)
+      e = cudaMemcpy2DAsync(in_dev, ci.dpitch, (const char *)p->in.host + ci.off * p->elt,
+                            ci.hpitch, ci.width, ci.height, cudaMemcpyHostToDevice, si);
+    if (e == cudaSuccess && p->out_read)
+      e = cudaMemcpy2DAsync(out_dev, co.dpitch, (const char *)p->out.host + co.off * p->elt,
+                            co.hpitch, co.width, co.height, cudaMemcpyHostToDevice, si);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[q][0], si);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, ev[q][0], 0);
+    if (e != cudaSuccess) {
+      st = b200_set_error(B200_ECUDA, "pipeline: panel copy-in failed");
+      break;
+    }
+    st = p->run(p->ctx, j0, cols, has_in ? in_dev : nullptr, ci.drs, ci.dcs, out_dev, co.drs,
+                co.dcs);
+    if (st != B200_OK) break;
+    e = cudaEventRecord(ev[q][1], sc);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(so, ev[q][1], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync((char *)p->out.host + co.off * p->elt, co.hpitch, out_dev, co.dpitch,
+                            co.width, co.height, cudaMemcpyDeviceToHost, so);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[q][2], so);
+    if (e != cudaSuccess) st = b200_set_error(B200_ECUDA, "pipeline: panel copy-out failed");
+  }
+  // Drain: the copy streams finish, then the buffers are released on sc.
+  cudaStreamSynchronize(si);
+  cudaStreamSynchronize(so);
+  const int sync = b200_stream_sync();
+  for (int q = 0; q < 2; ++q) {
+    b200_free(buf[q]);
+    for (int e = 0; e < 3; ++e)
+      if (ev[q][e]) cudaEventDestroy(ev[q][e]);
+  }
+  if (ready) cudaEventDestroy(ready);
+  return st != B200_OK ? st : sync;
 }
 
 // ---- public runtime controls (include/mublis_b200.h) ----------------------

@@ -102,6 +102,28 @@ def test_auto_form_matches_plain_error(lib):
     assert finite and err <= TOL["plain"](1024, 2.0 ** -24)
 
 
+def test_auto_form_fp64_picks_emulation_within_plain_error(lib):
+    """At 2048^3 "auto" runs FP64 GEMM on the modular form; its error against
+    double-double values of 512 sampled entries must stay within plain's
+    bound."""
+    n = 2048
+    a = orc.fill(n, n, np.float64, 12, 0)
+    b = orc.fill(n, n, np.float64, 12, 1)
+    c0 = orc.fill(n, n, np.float64, 12, 2)
+    rng = np.random.default_rng(4)
+    rows, cols = rng.integers(0, n, 512), rng.integers(0, n, 512)
+    hi, lo = orc.dd_gemm_entries(a, b, rows, cols, alpha=1.0, beta=0.5, c0=c0)
+    assert lib.mublis_b200_set_form(b"d", b"auto") == 0
+    c = c0.copy(order="F")
+    assert lib.mublis_dgemm(0, 0, n, n, n, 1.0, a.ctypes.data, 1, n, b.ctypes.data, 1, n, 0.5,
+                            c.ctypes.data, 1, n) == 0, mb.last_error(lib)
+    lib.mublis_b200_set_form(b"d", b"plain")
+    d = c[rows, cols] - (hi + lo)
+    den = np.linalg.norm(a) * np.linalg.norm(b) + 0.5 * np.linalg.norm(c0)
+    err = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
+    assert err <= 4 * n * 2.0 ** -53, err
+
+
 def test_wide_range_inputs_ozaki(lib):
     """The wide draw (|x| = m * 2^e, e in [-10, 10]) stresses the per-row
     scaling of the Ozaki split."""

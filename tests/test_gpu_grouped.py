@@ -172,3 +172,44 @@ def test_trsm_plan_replay(glib, p):
     for q in range(len(probs)):
         assert torch.equal(replay[q], keep[q][1])
     assert glib.mublis_b200_plan_destroy(plan) == 0
+
+
+def test_tuned_table_round_trip(glib, tmp_path):
+    """The autotuner's choices survive a save / reset / load cycle: a plan
+    created after loading the table launches no tuning trials; a table keyed
+    to another GPU loads nothing."""
+    torch = pytest.importorskip("torch")
+    probs, keep = make_gemm_set(torch, "s", 40, seed=9)
+    arr = (GemmProblem * len(probs))(*probs)
+    assert glib.mublis_b200_tune_reset() == 0
+
+    def plan_launches():
+        plan = ctypes.c_void_p()
+        n0 = glib.mublis_b200_launch_count()
+        assert glib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)) == 0
+        n1 = glib.mublis_b200_launch_count()
+        assert glib.mublis_b200_plan_destroy(plan) == 0
+        return n1 - n0
+
+    untuned = plan_launches()
+    path = tmp_path / "tune.txt"
+    assert glib.mublis_b200_tune_save(str(path).encode()) == 0, mb.last_error(glib)
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith("mublis_b200-tune ") and "driver=" in lines[0]
+    choices = [ln for ln in lines[1:] if ln.startswith("gemm ")]
+    assert choices
+
+    assert glib.mublis_b200_tune_reset() == 0
+    entries = ctypes.c_int(-1)
+    assert glib.mublis_b200_tune_load(str(path).encode(), ctypes.byref(entries)) == 0
+    assert entries.value == len(choices)
+    assert plan_launches() < untuned  # no trial launches once the table is loaded
+
+    other = tmp_path / "other.txt"
+    other.write_text("mublis_b200-tune Another_GPU sms=1 cc=1.0 driver=1 table=1\ngemm 0 0 0 1\n")
+    assert glib.mublis_b200_tune_reset() == 0
+    assert glib.mublis_b200_tune_load(str(other).encode(), ctypes.byref(entries)) == 0
+    assert entries.value == 0
+    missing = tmp_path / "missing.txt"
+    assert glib.mublis_b200_tune_load(str(missing).encode(), ctypes.byref(entries)) == 0
+    assert entries.value == 0
