@@ -246,8 +246,8 @@ int launch_simt_gemm<float>(const SimtGemmArgs<float> &a, cudaStream_t s) {
   switch (simt_variant(false)) {
   case 1: return launch_cfg<float, 128, 128, 2, 4, 4, 2>(a, s);
   case 2: return launch_cfg<float, 128, 128, 4, 2, 3, 1>(a, s);
-  case 3: return launch_cfg<float, 128, 128, 4, 2, 4, 2, true>(a, s);
-  default: return launch_cfg<float, 128, 128, 4, 2, 4, 2>(a, s);
+  case 3: return launch_cfg<float, 128, 128, 4, 2, 4, 2>(a, s);  // scalar fmaf
+  default: return launch_cfg<float, 128, 128, 4, 2, 4, 2, true>(a, s);  // packed: 52 -> 56 TF/s
   }
 }
 
