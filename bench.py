@@ -51,7 +51,6 @@ COL, NT, TR, UPPER, LOWER, NONUNIT, LEFT = 102, 111, 112, 121, 122, 131, 141
 ALPHA, BETA = 0.75, 0.25
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # SMs x FP64 FMA lanes x 2 x max clock
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs x FP32 FMA lanes x 2 x max clock
-LEAF = 64  # TRSM diagonal-block leaf size (rows) of the device solve
 
 
 def flops(routine: str, n: int) -> float:
@@ -70,20 +69,15 @@ def family_flops(n: int) -> float:
     return 2 * sum(flops(r, n) for r in ROUTINES)
 
 
-DIRECT_K = 256  # TRSM updates with k <= this read operands directly (no pack)
-
-
 def kernel_flops(n: int) -> dict:
     """Algorithmic flops of one step attributed to the kernel that executes
-    them.  The recursive TRSM of order n (a power of two) halves down to
-    LEAF-row diagonal blocks: updates of half-order h > DIRECT_K (sum of h =
-    n - 2*DIRECT_K) run on the packed GEMM kernel, the thinner updates (sum
-    2*DIRECT_K - LEAF) and the leaf solves (LEAF * n^2, done as products with
-    the inverted diagonal blocks) on the direct kernel."""
-    gemm_part = sum(flops(r, n) for r in ROUTINES if r != "trsm") + n * n * (n - 2 * DIRECT_K)
-    direct = float(n * n * 2 * DIRECT_K)
-    return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part, "dmma_dgemm": gemm_part,
-            "direct_sgemm": direct, "direct_dgemm": direct}
+    them.  Every routine, TRSM included, runs on the packed GEMM kernel: the
+    recursive TRSM's updates do m^2 n (1 - b/m) and its leaf products (the
+    inverted b x b diagonal blocks times B) cover the remaining m b n of the
+    triangle (they execute 2 m b n, twice the triangle's work, which is not
+    credited)."""
+    gemm_part = sum(flops(r, n) for r in ROUTINES)
+    return {"simt_sgemm": gemm_part, "simt_dgemm": gemm_part, "dmma_dgemm": gemm_part}
 
 
 def max_over_ranks(dist, torch, ms: float, world: int, device: str = "cuda") -> float:
@@ -352,6 +346,36 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
     return out
 
 
+def sides_study(torch, lib, n: int = 4096) -> dict:
+    """TRSM and TRMM for every side x uplo x transpose at m = n (device
+    operands, alpha 1, non-unit, A = U[0,1)/n + 1.5 I), TF/s credited with
+    m^2 n; mean of 2 event-timed calls after a warm-up."""
+    out = {}
+    for p, dt in (("s", torch.float32), ("d", torch.float64)):
+        a = torch.rand(n, n, dtype=dt, device="cuda") / n
+        a.diagonal().add_(1.5)
+        b0 = torch.rand(n, n, dtype=dt, device="cuda")
+        b = b0.clone()
+        for r in ("trsm", "trmm"):
+            fn = getattr(lib, f"cblas_{p}{r}")
+            for side, sname in ((LEFT, "left"), (LEFT + 1, "right")):
+                for uplo, uname in ((LOWER, "lower"), (UPPER, "upper")):
+                    for tr, tname in ((NT, "N"), (TR, "T")):
+                        call = lambda: fn(COL, side, uplo, tr, NONUNIT, n, n, 1.0,  # noqa: E731
+                                          ctypes.c_void_p(a.data_ptr()), n,
+                                          ctypes.c_void_p(b.data_ptr()), n)
+                        b.copy_(b0)
+                        call()
+                        ms = 0.0
+                        for _ in range(2):
+                            b.copy_(b0)
+                            ms += timed(torch, call, 1)
+                        out[f"{p}{r} {sname} {uname} {tname}"] = round(float(n) ** 3 / (ms / 2) / 1e9, 1)
+        del a, b, b0
+        torch.cuda.empty_cache()
+    return out
+
+
 def _log_uniform_int(rng, lo, hi, size):
     import numpy as np
     return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size))).astype(int)
@@ -568,6 +592,8 @@ def main():
     ap.add_argument("--only-forms", action="store_true",
                     help="run only the precision-form study (for profiler captures)")
     ap.add_argument("--forms-n", type=int, default=8192)
+    ap.add_argument("--only-sides", action="store_true",
+                    help="run only the TRSM/TRMM side x uplo x transpose study")
     ap.add_argument("--only-timed", action="store_true",
                     help="warm-up + timed steps only (for profiler launch lists)")
     args = ap.parse_args()
@@ -596,6 +622,11 @@ def main():
         lib.mublis_b200_set_form(p, b"plain")
     stream = torch.cuda.current_stream()
     mb.check(lib.mublis_b200_set_stream(ctypes.c_void_p(stream.cuda_stream)), lib)
+
+    if args.only_sides:
+        if rank == 0:
+            print(json.dumps({"sides_tflops": sides_study(torch, lib, args.n), "n": args.n}))
+        return
 
     if args.only_forms:
         if rank == 0:

@@ -94,8 +94,8 @@ extern "C" int mublis_b200_sgemm_noalloc(mublis_trans_t trans_a, mublis_trans_t 
     char msg[256];
     snprintf(msg, sizeof msg,
              "sgemm_noalloc: m=%d n=%d k=%d needs %ld scratch floats "
-             "((roundup(m,128) + roundup(n,128)) * roundup(k,16)); the maximum is %ld",
-             m, n, k, (mpad + npad) * kpad, NOALLOC_SCRATCH_FLOATS);
+             "((roundup(m,%d) + roundup(n,%d)) * roundup(k,%d)); the maximum is %ld",
+             m, n, k, (mpad + npad) * kpad, Cfg::BM, Cfg::BN, Cfg::BK, NOALLOC_SCRATCH_FLOATS);
     return b200_set_error(B200_EINVAL, msg);
   }
   float *scratch = nullptr;

@@ -8,16 +8,17 @@
 //   * recursive halving: solve the top half, update the bottom half with one
 //     GEMM (k = half the order, so it runs at GEMM speed), solve the bottom
 //     half (upper: mirror image);
-//   * leaves are the 256 x 256 diagonal blocks, inverted up front: one launch
+//   * leaves are the 512 x 512 diagonal blocks, inverted up front: one launch
 //     inverts every 64 x 64 diagonal block by substitution against the
 //     reciprocal diagonal (computed once and multiplied -- never divided --
-//     as the reference does), then two doubling steps of two batched
-//     (grouped) GEMM launches each build the 128- and 256-blocks,
+//     as the reference does), then three doubling steps of two batched
+//     (grouped) GEMM launches each build the 128-, 256- and 512-blocks,
 //     inv([A11 0; A21 A22]) = [inv11 0; -inv22 A21 inv11  inv22];
-//   * each leaf solve is then X_b = inv(A_bb) B_b, one 256-deep GEMM over all
+//   * each leaf solve is then X_b = inv(A_bb) B_b, one 512-deep GEMM over all
 //     right-hand sides (plain FP64/FP32: the diagonal blocks never use an
-//     emulated form), and every update is a GEMM of k >= 256 on the packed
-//     path (and the caller's form);
+//     emulated form), and every update is a GEMM of k >= 512 on the packed
+//     path (and the caller's form).  512-row leaves give those GEMMs at least
+//     128 output tiles of 128 x 128 for 148 SMs (256-row leaves gave 64);
 //   * the unit diagonal and the unstored triangle are never read.
 // alpha is applied once up front (the reference's alpha_eff on the first
 // block, trsm.c:96-97).
@@ -30,7 +31,7 @@
 namespace {
 
 constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
-constexpr int BIG = 256;  // inverted diagonal blocks the solve uses (leaves)
+constexpr int BIG = 512;  // inverted diagonal blocks the solve uses (leaves)
 constexpr int PER_BIG = BIG / LEAF;
 
 // One CTA per LEAF block: thread j computes column j of the inverse of the
