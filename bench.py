@@ -299,7 +299,7 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
     """Precision forms at m = n = k = n (8192 by default; one call each,
     event-timed)."""
     out = {}
-    for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6", "ozaki2"]),
+    for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6", "fp16x3", "ozaki2"]),
                          ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
         fill = getattr(lib, f"mublis_b200_fill_{p}")
         a, b, c = (torch.empty(n, n, dtype=dt, device="cuda") for _ in range(3))
@@ -565,7 +565,7 @@ def served_study(torch, lib, nreq: int = 400) -> dict:
                 "served": {"tflops": round(tot / span_v / 1e12, 2), "p50_ms": pct(lat_v, 50),
                            "p99_ms": pct(lat_v, 99), "batches": int(st.batches),
                            "batched_requests": int(st.batched_requests),
-                           "forms": "auto (bf16x6 / ozaki2 above crossover, else plain)"},
+                           "forms": "auto (fp16x3 / bf16x6 / ozaki2 above crossover, else plain)"},
                 "serialized_plain": {"tflops": round(tot / span_s / 1e12, 2),
                                      "p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99)},
                 "throughput_ratio": round(span_s / span_v, 2)}

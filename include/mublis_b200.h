@@ -34,12 +34,19 @@ void *mublis_b200_get_stream(void);
 
 /* Precision form used by the routines of one precision ('s' or 'd'):
  *   's': "plain" (FP32 FMA pipe), "bf16x3" (tcgen05, hi/lo split, 3
- *        products, FP32 accumulate), "bf16x6" (3-term split, 6 products)
- *   'd': "plain" (FP64 FMA pipe), "ozaki" or "ozaki:<slices>" (int8 slices,
- *        exact int32 tensor-core accumulation, FP64 recombination)
+ *        products, FP32 accumulate), "bf16x6" (3-term split, 6 products),
+ *        "fp16x3" (per-row/column scaled fp16 hi/lo split, 3 products)
+ *   'd': "plain" (FP64 tensor pipe, mma.sync .f64), "ozaki" or
+ *        "ozaki:<slices>" (int8 slices, exact int32 tensor-core
+ *        accumulation, FP64 recombination)
+ *   both: "ozaki2" or "ozaki2:<moduli>" (int8 residues modulo up to 16
+ *        moduli, exact int32 products, Chinese-remainder reconstruction;
+ *        default 16 moduli for FP64, 8 for FP32)
  *   both: "auto" -- per call, the fastest form whose error is no worse than
- *        plain: FP32 uses bf16x6 when min(m, n) and k are >= 512, FP64 uses
- *        ozaki:8 when min(m, n) and k are >= 4096, plain otherwise
+ *        plain: FP32 uses fp16x3 when min(m, n) >= 4096 and k >= 2048,
+ *        bf16x6 when min(m, n) and k are >= 512, FP64 uses
+ *        ozaki2 when min(m, n) and k are >= 1024 and m * n >= 2048^2,
+ *        plain otherwise
  * Also settable with MUBLIS_B200_SFORM / MUBLIS_B200_DFORM. */
 int mublis_b200_set_form(char dtype, const char *form);
 

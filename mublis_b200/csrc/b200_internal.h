@@ -38,10 +38,10 @@ enum { B200_F32 = 0, B200_F64 = 1 };
  * reconstruction (N in `slices`). */
 enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM_BF16X6 = 2,
        B200_FORM_OZAKI = 3, B200_FORM_POLICY = 4 /* "auto": per-call size crossover */,
-       B200_FORM_OZAKI2 = 5 };
+       B200_FORM_OZAKI2 = 5, B200_FORM_FP16X3 = 6 /* FP32 via scaled fp16 hi/lo, 3 products */ };
 
-/* Parse a form name ("plain", "bf16x3", "bf16x6", "ozaki[:s]", "ozaki2[:N]",
- * "auto"); B200_FORM_AUTO for anything else.  *slices gets s or N when
+/* Parse a form name ("plain", "bf16x3", "bf16x6", "fp16x3", "ozaki[:s]",
+ * "ozaki2[:N]", "auto"); B200_FORM_AUTO for anything else.  *slices gets s or N when
  * given (slices may be NULL). */
 int b200_parse_form(const char *s, int *slices);
 
@@ -66,6 +66,9 @@ typedef struct {
   mublis_l3_product_t product;
   int form;   /* B200_FORM_* or AUTO (library default for the dtype) */
   int slices; /* Ozaki slice count, 0 = library default */
+  long policy_n; /* n the "auto" policy decides on (0: n).  A column panel of a
+                  * larger call carries the call's n, so every panel takes the
+                  * form the whole call would. */
 } b200_l3_desc_t;
 
 /* Left-side solve op(A) X = alpha B, already normalised by the host layer
@@ -82,6 +85,7 @@ typedef struct {
   int unit_diag;
   int form;
   int slices;
+  long policy_n; /* as in b200_l3_desc_t, passed to the update products */
 } b200_trsm_desc_t;
 
 /* runtime.cu */
@@ -94,6 +98,8 @@ int b200_stream_sync(void);
 int b200_alloc(void **p, size_t bytes);
 void b200_free(void *p);
 int b200_set_error(int code, const char *where);
+/* Multiprocessor count of the calling thread's current device (cached). */
+int b200_sm_count(void);
 const char *b200_last_error(void);
 int b200_get_default_form(int dtype);
 int b200_set_default_form(int dtype, int form, int slices);

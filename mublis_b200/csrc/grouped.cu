@@ -254,15 +254,7 @@ enum { TILE_32 = 0, TILE_64 = 1, TILE_128x64 = 2, TILE_128 = 3, TILE_VARIANTS = 
 const int kTileBM[TILE_VARIANTS] = {32, 64, 128, 128};
 const int kTileBN[TILE_VARIANTS] = {32, 64, 64, 128};
 
-int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
-  }
-  return sms;
-}
+int sm_count() { return b200_sm_count(); }
 
 template <typename T>
 int launch_gemm_variant(int variant, const GemmEntry *dtable, int nprob, int tiles,

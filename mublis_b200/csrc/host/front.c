@@ -111,6 +111,7 @@ static int l3_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, lon
                     void *out_dev, long out_rs, long out_cs) {
   (void)j0;
   b200_l3_desc_t d = *(const b200_l3_desc_t *)ctx;
+  if (d.policy_n <= 0) d.policy_n = d.n;
   d.n = (int)cols;
   d.b[0] = in_dev ? in_dev : out_dev; /* in place when there is no separate input */
   d.rs_b[0] = in_dev ? in_rs : out_rs;
@@ -125,6 +126,7 @@ static int trsm_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, l
                       void *out_dev, long out_rs, long out_cs) {
   (void)j0, (void)in_dev, (void)in_rs, (void)in_cs;
   b200_trsm_desc_t d = *(const b200_trsm_desc_t *)ctx;
+  if (d.policy_n <= 0) d.policy_n = d.n;
   d.n = (int)cols;
   d.b = out_dev;
   d.rs_b = out_rs;

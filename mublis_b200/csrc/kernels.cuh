@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 
@@ -48,9 +49,18 @@ enum PackXform {
   PACK_BF16_SPLIT = 1,   // f32 -> `terms` bf16 planes (hi, lo[, lo2])
   PACK_INT8_SLICES = 2,  // f64 -> `terms` int8 planes of 7-bit slices of
                          // x * 2^(7 - e), e from the row/column abs-max
-  PACK_INT8_MODULI = 3   // f64 -> `terms` int8 planes: the symmetric residues
+  PACK_INT8_MODULI = 3,  // f64 -> `terms` int8 planes: the symmetric residues
                          // of X = rint(x * 2^(bits - e)) modulo each modulus
+  PACK_FP16_SPLIT = 4    // f32 -> 2 fp16 planes of xs = x * 2^(15 - e) (e from
+                         // the row/column abs-max, |xs| < 2^15): hi = rn(xs),
+                         // lo = rn(xs - hi)
 };
+
+// fp16 split scaling: the row/column maximum lands just below 2^15, so that
+// lo = rn(xs - hi) (about 2^-11 |xs|) stays a normal fp16 number for every
+// element down to 2^-18 of its row's maximum (fp16 normals start at 2^-14;
+// the tensor cores ran the product noticeably slower on subnormal halves).
+constexpr int B200_FP16_SCALE_EXP = 15;
 
 // Pairwise coprime moduli (<= 256) of the modular (CRT) Ozaki form and the
 // constants that reduce an integer modulo each of them without division:
@@ -89,12 +99,30 @@ template <typename T>
 int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
                   unsigned long long *absmax, cudaStream_t s);
 
+// exps[i] = b200_scale_exp(absmax[i]) for i < count: the epilogues read one
+// int per row / column instead of a 64-bit abs-max and its frexp.
+int launch_scale_exps(const unsigned long long *absmax, int *exps, long count, cudaStream_t s);
+
 // Exponent e with max|x| < 2^e (frexp), 0 for an all-zero row.
 __device__ inline int b200_scale_exp(unsigned long long absmax_bits) {
   if (absmax_bits == 0) return 0;
   int e;
   frexp(__longlong_as_double((long long)absmax_bits), &e);
   return e;
+}
+
+// x * 2^e rounded once.
+//  * float: the product is formed exactly in FP64 and rounded once to float;
+//    valid for -1022 <= e <= 1023 (the fp16x3 epilogue's e = e_i + f_j - 30
+//    stays within [-330, 230] for FP32 inputs).
+//  * double: one multiply by the exact power of two where 2^e is a normal
+//    number, else ldexp.
+__device__ __forceinline__ float b200_pow2_scale(float x, int e) {
+  return (float)((double)x * __longlong_as_double((long long)(e + 1023) << 52));
+}
+__device__ __forceinline__ double b200_pow2_scale(double x, int e) {
+  return e >= -1022 && e <= 1023 ? x * __longlong_as_double((long long)(e + 1023) << 52)
+                                 : ldexp(x, e);
 }
 
 template <typename T>

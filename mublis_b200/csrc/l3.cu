@@ -32,13 +32,22 @@ namespace {
 int resolve_form(const b200_l3_desc_t *d) {
   int f = d->form == B200_FORM_AUTO ? b200_get_default_form(d->dtype) : d->form;
   if (f == B200_FORM_POLICY) {
-    const long m = d->m, n = d->n, k = (long)d->k * d->npairs;
+    const long m = d->m, n = d->policy_n > 0 ? d->policy_n : d->n;
+    const long k = (long)d->k * d->npairs;
     const long mn = m < n ? m : n;
-    if (d->dtype == B200_F32) return mn >= 512 && k >= 512 ? B200_FORM_BF16X6 : B200_FORM_PLAIN;
+    // FP32: fp16x3 (normwise error ~0.6x plain) where it is at least as fast
+    // as bf16x6 (error ~1.0x plain): from 4096 on (at 2048^3 its abs-max
+    // pass and slower fp16 MMAs leave it ~10% behind).
+    if (d->dtype == B200_F32) {
+      if (mn >= 4096 && k >= 2048) return B200_FORM_FP16X3;
+      return mn >= 512 && k >= 512 ? B200_FORM_BF16X6 : B200_FORM_PLAIN;
+    }
     return mn >= 1024 && k >= 1024 && m * n >= 2048L * 2048 ? B200_FORM_OZAKI2 : B200_FORM_PLAIN;
   }
   if (d->dtype == B200_F32 && f == B200_FORM_OZAKI) f = B200_FORM_PLAIN;
-  if (d->dtype == B200_F64 && (f == B200_FORM_BF16X3 || f == B200_FORM_BF16X6)) f = B200_FORM_PLAIN;
+  if (d->dtype == B200_F64 &&
+      (f == B200_FORM_BF16X3 || f == B200_FORM_BF16X6 || f == B200_FORM_FP16X3))
+    f = B200_FORM_PLAIN;
   return f;
 }
 
@@ -208,7 +217,8 @@ extern "C" int b200_l3_run(const b200_l3_desc_t *d) {
     return b200_scale_strided(d->dtype, d->m, d->n, d->beta, d->c, d->rs_c, d->cs_c,
                               d->product.domain.ji);
   const int form = resolve_form(d);
-  if (form == B200_FORM_BF16X3 || form == B200_FORM_BF16X6) return tc_run_bf16(d, form);
+  if (form == B200_FORM_BF16X3 || form == B200_FORM_BF16X6 || form == B200_FORM_FP16X3)
+    return tc_run_bf16(d, form);
   if (form == B200_FORM_OZAKI || form == B200_FORM_OZAKI2) {
     b200_l3_desc_t e = *d;
     e.form = form;

@@ -102,6 +102,12 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
         out[off + t * o.plane_stride] = (int8_t)(int)q;
         r = (r - q) * 128.0;
       }
+    } else if (o.xform == PACK_FP16_SPLIT) {
+      __half *out = (__half *)o.out;
+      const float xs = ldexpf((float)val, B200_FP16_SCALE_EXP - b200_scale_exp(o.absmax[mn]));
+      const __half hi = __float2half_rn(xs);
+      out[off] = hi;
+      out[off + o.plane_stride] = __float2half_rn(xs - __half2float(hi));
     } else if (o.xform == PACK_INT8_MODULI) {
       // X = rint(x * 2^(bits - e)) is an integer with |X| <= 2^bits <= 2^56,
       // exact in FP64.  Cut it into 19-bit pieces X = x2 2^38 + x1 2^19 + x0
@@ -160,6 +166,18 @@ __device__ __forceinline__ void kmajor_store8(const PackOut &o, long mn, long of
     if (o.terms > 2)
       *reinterpret_cast<uint4 *>(out + off + 2 * o.plane_stride) =
           *reinterpret_cast<const uint4 *>(l2);
+  } else if (o.xform == PACK_FP16_SPLIT) {
+    __half *out = (__half *)o.out;
+    const int sh = B200_FP16_SCALE_EXP - b200_scale_exp(o.absmax[mn]);
+    __align__(16) __half h[8], l[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float xs = ldexpf((float)v[j], sh);
+      h[j] = __float2half_rn(xs);
+      l[j] = __float2half_rn(xs - __half2float(h[j]));
+    }
+    *reinterpret_cast<uint4 *>(out + off) = *reinterpret_cast<const uint4 *>(h);
+    *reinterpret_cast<uint4 *>(out + off + o.plane_stride) = *reinterpret_cast<const uint4 *>(l);
   } else if (o.xform == PACK_INT8_MODULI) {
     int8_t *out = (int8_t *)o.out;
     const int sh = o.bits - b200_scale_exp(o.absmax[mn]);
@@ -237,34 +255,152 @@ __global__ void __launch_bounds__(256) pack_kmajor_kernel(PackView v, bool b_sid
   kmajor_store8<T>(o, mn, mn * o.ld + kk, vals);
 }
 
+// Abs-max per row of op(A) / column of op(B), for the power-of-two scaling
+// of the fp16 and Ozaki forms.  Every block reduces a range of k in
+// registers and issues one atomicMax (on the bits of a non-negative double,
+// which order like the values) per row it covers.  The host sizes the k
+// range so the grid fills the SMs several times over.
+//
+// absmax_kernel is the general form (structured and masked operands, any
+// strides): 32 rows per block, loads along whichever index is contiguous.
 template <typename T>
 __global__ void __launch_bounds__(256) absmax_kernel(PackView v, bool b_side, long mn_len,
-                                                     long k_len, bool mn_fast_load,
+                                                     long k_len, long kch, bool mn_fast_load,
                                                      unsigned long long *absmax) {
-  __shared__ double tile[32][33];  // [kk_local][mn_local]
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const long mn_base = (long)blockIdx.x * 32, kk_base = (long)blockIdx.y * 32;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    int a = tx, b = ty + 8 * q;
-    int mn_l = mn_fast_load ? a : b, kk_l = mn_fast_load ? b : a;
-    long mn = mn_base + mn_l, kk = kk_base + kk_l;
-    double val = 0.0;
-    if (mn < mn_len && kk < k_len) {
-      long r = b_side ? kk : mn, c = b_side ? mn : kk;
-      val = fabs((double)load_logical<T>(v, r, c));
-    }
-    tile[kk_l][mn_l] = val;
-  }
-  __syncthreads();
-  if (ty == 0) {
+  __shared__ double part[8][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const long mn_base = (long)blockIdx.x * 32, k0 = (long)blockIdx.y * kch;
+  const long k1 = k0 + kch < k_len ? k0 + kch : k_len;
+  if (mn_fast_load) {
+    const long mn = mn_base + tx;
     double mx = 0.0;
-#pragma unroll 8
-    for (int kk = 0; kk < 32; ++kk) mx = fmax(mx, tile[kk][tx]);
-    long mn = mn_base + tx;
-    if (mn < mn_len && mx > 0.0)
+    if (mn < mn_len) {
+#pragma unroll 4
+      for (long kk = k0 + ty; kk < k1; kk += 8) {
+        long r = b_side ? kk : mn, c = b_side ? mn : kk;
+        mx = fmax(mx, fabs((double)load_logical<T>(v, r, c)));
+      }
+    }
+    part[ty][tx] = mx;
+    __syncthreads();
+    if (ty == 0) {
+#pragma unroll
+      for (int q = 1; q < 8; ++q) mx = fmax(mx, part[q][tx]);
+      if (mn < mn_len && mx > 0.0)
+        atomicMax(&absmax[mn], (unsigned long long)__double_as_longlong(mx));
+    }
+    return;
+  }
+#pragma unroll 1
+  for (int q = 0; q < 4; ++q) {
+    const long mn = mn_base + ty + 8 * q;
+    if (mn >= mn_len) break;  // uniform across the warp
+    double mx = 0.0;
+#pragma unroll 4
+    for (long kk = k0 + tx; kk < k1; kk += 32) {
+      long r = b_side ? kk : mn, c = b_side ? mn : kk;
+      mx = fmax(mx, fabs((double)load_logical<T>(v, r, c)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (tx == 0 && mx > 0.0)
       atomicMax(&absmax[mn], (unsigned long long)__double_as_longlong(mx));
   }
+}
+
+// 16-byte vector of T and its element-wise |.|-max fold.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+  using V = float4;
+  static constexpr int N = 4;
+  __device__ static void fold(double (&m)[4], const V &x) {
+    m[0] = fmax(m[0], fabs((double)x.x)); m[1] = fmax(m[1], fabs((double)x.y));
+    m[2] = fmax(m[2], fabs((double)x.z)); m[3] = fmax(m[3], fabs((double)x.w));
+  }
+  __device__ static double fold1(const V &x) {
+    return fmax(fmax(fabs((double)x.x), fabs((double)x.y)),
+                fmax(fabs((double)x.z), fabs((double)x.w)));
+  }
+};
+template <> struct Vec16<double> {
+  using V = double2;
+  static constexpr int N = 2;
+  __device__ static void fold(double (&m)[2], const V &x) {
+    m[0] = fmax(m[0], fabs(x.x)); m[1] = fmax(m[1], fabs(x.y));
+  }
+  __device__ static double fold1(const V &x) { return fmax(fabs(x.x), fabs(x.y)); }
+};
+
+// absmax_dense_kernel: a general (unstructured, unmasked) operand whose
+// rows (MN_CONTIG: the mn index) or k index has unit stride, 16-byte aligned
+// base and a leading stride that is a multiple of 16 bytes; every load is a
+// 16-byte vector.
+//  * MN_CONTIG: lane l holds VN consecutive mn, the 8 warps stride over k;
+//    a block covers 32*VN mn.
+//  * otherwise: each warp reduces one mn over the block's k range, lane l
+//    reading VN consecutive k; a block covers 8 mn.
+template <typename T, bool MN_CONTIG>
+__global__ void __launch_bounds__(256) absmax_dense_kernel(const T *x, long ld, long mn_len,
+                                                           long k_len, long kch,
+                                                           unsigned long long *absmax) {
+  using VT = Vec16<T>;
+  using V = typename VT::V;
+  constexpr int VN = VT::N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long k0 = (long)blockIdx.y * kch;
+  const long k1 = k0 + kch < k_len ? k0 + kch : k_len;
+  if (MN_CONTIG) {
+    __shared__ double part[8][32 * VN];
+    const long mn0 = (long)blockIdx.x * (32 * VN) + lane * VN;
+    double m[VN];
+#pragma unroll
+    for (int e = 0; e < VN; ++e) m[e] = 0.0;
+    if (mn0 + VN <= mn_len) {
+#pragma unroll 4
+      for (long kk = k0 + warp; kk < k1; kk += 8) VT::fold(m, *(const V *)(x + kk * ld + mn0));
+    } else if (mn0 < mn_len) {
+      for (long kk = k0 + warp; kk < k1; kk += 8)
+        for (int e = 0; e < VN && mn0 + e < mn_len; ++e)
+          m[e] = fmax(m[e], fabs((double)x[kk * ld + mn0 + e]));
+    }
+#pragma unroll
+    for (int e = 0; e < VN; ++e) part[warp][lane * VN + e] = m[e];
+    __syncthreads();
+    if (threadIdx.x < 32 * VN) {
+      const long mn = (long)blockIdx.x * (32 * VN) + threadIdx.x;
+      double mx = part[0][threadIdx.x];
+#pragma unroll
+      for (int q = 1; q < 8; ++q) mx = fmax(mx, part[q][threadIdx.x]);
+      if (mn < mn_len && mx > 0.0)
+        atomicMax(&absmax[mn], (unsigned long long)__double_as_longlong(mx));
+    }
+  } else {
+    const long mn = (long)blockIdx.x * 8 + warp;
+    if (mn >= mn_len) return;  // whole warp
+    const T *row = x + mn * ld;
+    double mx = 0.0;
+#pragma unroll 8
+    for (long kk = k0 + lane * VN; kk < k1; kk += 32 * VN) {
+      if (kk + VN <= k1) {
+        mx = fmax(mx, VT::fold1(*(const V *)(row + kk)));
+      } else {
+        for (long t = kk; t < k1; ++t) mx = fmax(mx, fabs((double)row[t]));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0 && mx > 0.0)
+      atomicMax(&absmax[mn], (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+// Largest power-of-two k range (between lo and hi) that still gives at
+// least 8 blocks per SM.
+long absmax_kch(long blocks_x, long k_len, long lo, long hi) {
+  const long want = 8L * b200_sm_count();
+  long kch = hi;
+  while (kch > lo && blocks_x * b200_ceil_div(k_len, kch) < want) kch >>= 1;
+  return kch;
 }
 
 }  // namespace
@@ -275,11 +411,51 @@ int launch_absmax(const PackView &v, bool b_side, long mn_len, long k_len,
   if (mn_len <= 0 || k_len <= 0) return B200_OK;
   long mn_stride = b_side ? v.cs : v.rs;
   long kk_stride = b_side ? v.rs : v.cs;
-  bool mn_fast = labs(mn_stride) <= labs(kk_stride);
-  dim3 grid((unsigned)b200_ceil_div(mn_len, 32), (unsigned)b200_ceil_div(k_len, 32));
-  if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
   B200ProfScope prof("absmax", s);
-  absmax_kernel<T><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, mn_fast, absmax);
+  constexpr int VN = 16 / sizeof(T);
+  const bool dense = v.struc == MUBLIS_STRUC_GENERAL && v.mask_rel != MUBLIS_L3_LOWER &&
+                     v.mask_rel != MUBLIS_L3_UPPER && ((uintptr_t)v.x & 15) == 0;
+  if (dense && mn_stride == 1 && kk_stride > 0 && kk_stride % VN == 0) {
+    const long bx = b200_ceil_div(mn_len, 32 * VN);
+    const long kch = absmax_kch(bx, k_len, 64, 2048);
+    dim3 grid((unsigned)bx, (unsigned)b200_ceil_div(k_len, kch));
+    if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
+    absmax_dense_kernel<T, true><<<grid, 256, 0, s>>>((const T *)v.x, kk_stride, mn_len, k_len,
+                                                      kch, absmax);
+    B200_LAUNCH_CHECK();
+    return B200_OK;
+  }
+  if (dense && kk_stride == 1 && mn_stride > 0 && mn_stride % VN == 0) {
+    const long bx = b200_ceil_div(mn_len, 8);
+    const long kch = absmax_kch(bx, k_len, 32 * VN, 4096);
+    dim3 grid((unsigned)bx, (unsigned)b200_ceil_div(k_len, kch));
+    if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
+    absmax_dense_kernel<T, false><<<grid, 256, 0, s>>>((const T *)v.x, mn_stride, mn_len, k_len,
+                                                       kch, absmax);
+    B200_LAUNCH_CHECK();
+    return B200_OK;
+  }
+  const bool mn_fast = labs(mn_stride) <= labs(kk_stride);
+  const long bx = b200_ceil_div(mn_len, 32);
+  const long kch = absmax_kch(bx, k_len, 64, 1024);
+  dim3 grid((unsigned)bx, (unsigned)b200_ceil_div(k_len, kch));
+  if (grid.y > 65535) return b200_set_error(B200_EINVAL, "absmax: k extent too large");
+  absmax_kernel<T><<<grid, dim3(32, 8), 0, s>>>(v, b_side, mn_len, k_len, kch, mn_fast, absmax);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
+namespace {
+__global__ void scale_exps_kernel(const unsigned long long *absmax, int *exps, long count) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) exps[i] = b200_scale_exp(absmax[i]);
+}
+}  // namespace
+
+int launch_scale_exps(const unsigned long long *absmax, int *exps, long count, cudaStream_t s) {
+  if (count <= 0) return B200_OK;
+  B200ProfScope prof("absmax", s);
+  scale_exps_kernel<<<(unsigned)b200_ceil_div(count, 256), 256, 0, s>>>(absmax, exps, count);
   B200_LAUNCH_CHECK();
   return B200_OK;
 }

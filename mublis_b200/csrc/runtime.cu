@@ -69,7 +69,7 @@ void do_init() {
   int sf = b200_parse_form(getenv("MUBLIS_B200_SFORM"), &sslices);
   int df = b200_parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
   if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6 ||
-      sf == B200_FORM_OZAKI2 || sf == B200_FORM_POLICY)
+      sf == B200_FORM_FP16X3 || sf == B200_FORM_OZAKI2 || sf == B200_FORM_POLICY)
     g_default_form[B200_F32] = sf;
   if (df == B200_FORM_PLAIN || df == B200_FORM_OZAKI || df == B200_FORM_OZAKI2 ||
       df == B200_FORM_POLICY)
@@ -171,11 +171,25 @@ int b200_set_error(int code, const char *where) {
 
 const char *b200_last_error(void) { return t_error; }
 
+int b200_sm_count(void) {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  int sms = cache[dev].load(std::memory_order_relaxed);
+  if (!sms) {
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+      sms = 148;
+    cache[dev].store(sms, std::memory_order_relaxed);
+  }
+  return sms;
+}
+
 int b200_parse_form(const char *s, int *slices) {
   if (!s || !*s) return B200_FORM_AUTO;
   if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
   if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
   if (!strcmp(s, "bf16x6")) return B200_FORM_BF16X6;
+  if (!strcmp(s, "fp16x3")) return B200_FORM_FP16X3;
   if (!strcmp(s, "auto")) return B200_FORM_POLICY;
   const bool mod = !strncmp(s, "ozaki2", 6);
   if (mod || !strncmp(s, "ozaki", 5)) {
@@ -195,7 +209,8 @@ int b200_get_default_slices(int dtype) { return g_default_slices[dtype == B200_F
 
 int b200_set_default_form(int dtype, int form, int slices) {
   if (dtype == B200_F32 && form != B200_FORM_PLAIN && form != B200_FORM_BF16X3 &&
-      form != B200_FORM_BF16X6 && form != B200_FORM_OZAKI2 && form != B200_FORM_POLICY)
+      form != B200_FORM_BF16X6 && form != B200_FORM_FP16X3 && form != B200_FORM_OZAKI2 &&
+      form != B200_FORM_POLICY)
     return B200_EINVAL;
   if (dtype == B200_F64 && form != B200_FORM_PLAIN && form != B200_FORM_OZAKI &&
       form != B200_FORM_OZAKI2 && form != B200_FORM_POLICY)

@@ -123,7 +123,7 @@ size_t scratch_estimate(const Req &r) {
   int f = d.form;
   if (f == B200_FORM_POLICY) f = r.dtype == B200_F64 ? B200_FORM_OZAKI2 : B200_FORM_BF16X6;
   if (f == B200_FORM_BF16X6) return 3 * (mp + np) * kp * 2;
-  if (f == B200_FORM_BF16X3) return 2 * (mp + np) * kp * 2;
+  if (f == B200_FORM_BF16X3 || f == B200_FORM_FP16X3) return 2 * (mp + np) * kp * 2 + 8 * (mp + np);
   if (f == B200_FORM_OZAKI) return 12 * (mp + np) * kp + 148 * 256 * 256 * 8;
   if (f == B200_FORM_OZAKI2) return 16 * (mp + np) * kp + 148 * 16 * 256 * 256;
   return (mp + np) * kp * elt;

@@ -138,6 +138,9 @@ struct Bf16Params {
   float *c;
   long rs_c, cs_c;
   int *err;
+  // fp16 form: bits of max |x| per row of op(A) / column of op(B); the
+  // planes hold x * 2^-e, so the result is scaled back by 2^(e_i + f_j).
+  const int *aexp, *bexp;  // fp16x3: row / column scale exponents
 };
 
 template <int TERMS, int STAGES>
@@ -154,7 +157,7 @@ struct Bf16Cfg {
   static constexpr uint32_t TMEM_COLS = 512;
 };
 
-template <int TERMS, int STAGES>
+template <int TERMS, int STAGES, bool F16 = false>
 __global__ void __launch_bounds__(384, 1)
     tc_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    Bf16Params p) {
@@ -233,7 +236,7 @@ __global__ void __launch_bounds__(384, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
-    constexpr uint32_t IDESC = tc::idesc_bf16(C::BM, C::BN);
+    constexpr uint32_t IDESC = F16 ? tc::idesc_f16(C::BM, C::BN) : tc::idesc_bf16(C::BM, C::BN);
     int stage = 0, acc = 0;
     uint32_t phase = 0, acc_phase = 0;
     bool ok = true, any = false;
@@ -331,14 +334,33 @@ __global__ void __launch_bounds__(384, 1)
       }
       if (!ok) break;
       if (row_ok) {
+        // In batches of 16 columns: the batch's loads (C, and the column
+        // scales of fp16x3) are issued before its stores.  A load / store
+        // chain per element pays one memory round trip each, and while this
+        // store runs the MMAs of the next tile stall after two windows.
+        const int ei = F16 ? p.aexp[gi] : 0;
+        float *crow = p.c + gi * p.rs_c;
 #pragma unroll
-        for (int j = 0; j < C::HALF; ++j) {
-          const long gj = gj0 + j;
-          if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
-          float *cij = p.c + gi * p.rs_c + gj * p.cs_c;
-          float v = p.alpha * run[j];
-          if (p.beta != 0.f) v = fmaf(p.beta, *cij, v);
-          *cij = v;
+        for (int j0 = 0; j0 < C::HALF; j0 += 16) {
+          float cv[16];
+          int sc[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long gj = gj0 + j0 + j;
+            const bool in = gj < w.n && b200_rel(w.ji, gj, gi);
+            cv[j] = in && p.beta != 0.f ? crow[gj * p.cs_c] : 0.f;
+            sc[j] = F16 && in ? p.bexp[gj] : 0;
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long gj = gj0 + j0 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            float v = F16 ? p.alpha * b200_pow2_scale(run[j0 + j],
+                                                      ei + sc[j] - 2 * B200_FP16_SCALE_EXP)
+                          : p.alpha * run[j0 + j];
+            if (p.beta != 0.f) v = fmaf(p.beta, cv[j], v);
+            crow[gj * p.cs_c] = v;
+          }
         }
       }
     }
@@ -352,21 +374,20 @@ __global__ void __launch_bounds__(384, 1)
   }
 }
 
-template <int TERMS, int STAGES>
+template <int TERMS, int STAGES, bool F16 = false>
 int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &p,
                 cudaStream_t s) {
   using C = Bf16Cfg<TERMS, STAGES>;
-  auto kern = tc_bf16_kernel<TERMS, STAGES>;
+  auto kern = tc_bf16_kernel<TERMS, STAGES, F16>;
   static bool configured = false;
   if (!configured) {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
     configured = true;
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const int sms = b200_sm_count();
   int tiles = p.w.tiles_m * p.w.tiles_n;
   int grid = tiles < sms ? tiles : sms;
-  B200ProfScope prof(TERMS == 2 ? "tc_bf16x3" : "tc_bf16x6", s);
+  B200ProfScope prof(F16 ? "tc_fp16x3" : (TERMS == 2 ? "tc_bf16x3" : "tc_bf16x6"), s);
   kern<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);
   B200_LAUNCH_CHECK();
   return B200_OK;
@@ -375,9 +396,17 @@ int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &
 }  // namespace
 
 // Packs the FP32 operands into TERMS bf16 planes (K-major, padded) and runs
-// the tcgen05 kernel.
+// the tcgen05 kernel.  The fp16x3 form (Ootomo and Yokota's FP16 split with
+// per-row / per-column power-of-two scaling) scales row i of op(A) by
+// 2^(15 - e_i) and column j of op(B) by 2^(15 - f_j) so that |x| < 2^15,
+// splits into fp16 hi = rn(x) and lo = rn(x - hi) (11 + 11 significant
+// bits, both normal fp16 for elements down to 2^-18 of the maximum), runs
+// the same three products as bf16x3 (hi hi + hi lo + lo hi, FP32
+// accumulation drained every 256 k) and scales each result by
+// 2^(e_i + f_j - 30).
 int tc_run_bf16(const b200_l3_desc_t *d, int form) {
   if (d->dtype != B200_F32) return b200_set_error(B200_EINVAL, "bf16 forms are FP32-only");
+  const bool f16 = form == B200_FORM_FP16X3;
   const int terms = form == B200_FORM_BF16X6 ? 3 : 2;
   constexpr int BM = 128, BN = 256, BK = 32;
   cudaStream_t s = b200_cur_stream();
@@ -386,20 +415,40 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
   const long kpad = b200_round_up(ktot, BK);
   if (terms * (mpad > npad ? mpad : npad) > 0x7fffffffL)
     return b200_set_error(B200_EINVAL, "bf16 form: operand too large for 32-bit TMA rows");
-  void *ap = nullptr, *bp = nullptr;
+  void *ap = nullptr, *bp = nullptr, *amax = nullptr;
   B200_TRY(b200_alloc(&ap, sizeof(uint16_t) * terms * mpad * kpad));
   int st = b200_alloc(&bp, sizeof(uint16_t) * terms * npad * kpad);
   const mublis_l3_product_t &pr = d->product;
+  PackView va[2], vb[2];
+  for (int t = 0; t < d->npairs; ++t) {
+    va[t] = PackView{d->a[t], d->rs_a[t], d->cs_a[t], (int)pr.a.struc, (int)pr.a.uplo,
+                     (int)pr.a.diag, (int)pr.domain.pi};
+    vb[t] = PackView{d->b[t], d->rs_b[t], d->cs_b[t], (int)pr.b.struc, (int)pr.b.uplo,
+                     (int)pr.b.diag, (int)pr.domain.jp};
+  }
+  unsigned long long *am = nullptr, *bm = nullptr;
+  int *ae = nullptr;
+  if (f16 && st == B200_OK) {  // scales over the whole (concatenated) k
+    st = b200_alloc(&amax, (sizeof(unsigned long long) + sizeof(int)) * (mpad + npad));
+    am = (unsigned long long *)amax;
+    bm = am + mpad;
+    ae = (int *)(am + mpad + npad);
+    if (st == B200_OK &&
+        cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * (mpad + npad), s) != cudaSuccess)
+      st = b200_set_error(B200_ECUDA, "memset failed");
+    for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
+      st = launch_absmax<float>(va[t], false, d->m, d->k, am, s);
+      if (st == B200_OK) st = launch_absmax<float>(vb[t], true, d->n, d->k, bm, s);
+    }
+    if (st == B200_OK) st = launch_scale_exps(am, ae, mpad + npad, s);
+  }
+  const int xform = f16 ? PACK_FP16_SPLIT : PACK_BF16_SPLIT;
   for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
     long kk0 = (long)t * d->k, kk1 = t + 1 == d->npairs ? kpad : kk0 + d->k;
-    PackView va{d->a[t], d->rs_a[t], d->cs_a[t], (int)pr.a.struc, (int)pr.a.uplo,
-                (int)pr.a.diag, (int)pr.domain.pi};
-    PackView vb{d->b[t], d->rs_b[t], d->cs_b[t], (int)pr.b.struc, (int)pr.b.uplo,
-                (int)pr.b.diag, (int)pr.domain.jp};
-    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, PACK_BF16_SPLIT, terms, nullptr};
-    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, PACK_BF16_SPLIT, terms, nullptr};
-    st = launch_pack<float>(va, false, d->m, d->k, mpad, kk0, kk1, oa, s);
-    if (st == B200_OK) st = launch_pack<float>(vb, true, d->n, d->k, npad, kk0, kk1, ob, s);
+    PackOut oa{ap, kpad, mpad * kpad, PACK_K_MAJOR, xform, terms, am};
+    PackOut ob{bp, kpad, npad * kpad, PACK_K_MAJOR, xform, terms, bm};
+    st = launch_pack<float>(va[t], false, d->m, d->k, mpad, kk0, kk1, oa, s);
+    if (st == B200_OK) st = launch_pack<float>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
   }
   CUtensorMap ta, tb;
   if (st == B200_OK) st = b200_make_tmap(&ta, ap, 1, kpad, terms * mpad, BK, BM, 64);
@@ -426,10 +475,14 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
     p.rs_c = d->rs_c;
     p.cs_c = d->cs_c;
     p.err = b200_device_error_word();
-    st = terms == 2 ? launch_bf16<2, 4>(ta, tb, p, s) : launch_bf16<3, 3>(ta, tb, p, s);
+    p.aexp = ae;
+    p.bexp = ae ? ae + mpad : nullptr;
+    st = f16 ? launch_bf16<2, 4, true>(ta, tb, p, s)
+             : (terms == 2 ? launch_bf16<2, 4>(ta, tb, p, s) : launch_bf16<3, 3>(ta, tb, p, s));
   }
   b200_free(ap);
   b200_free(bp);
+  b200_free(amax);
   return st;
 }
 
@@ -501,7 +554,7 @@ struct OzParams {
   long rs_c, cs_c;
   void *work;  // slices: gridDim.x tiles of 256 x 256 doubles;
                // moduli: gridDim.x x N x 256 x 256 residue bytes
-  const unsigned long long *amax, *bmax;
+  const int *aexp, *bexp;  // row / column scale exponents
   int *err;
   OzCrt crt;
 };
@@ -697,7 +750,7 @@ __global__ void __launch_bounds__(384, 1)
       w.krange(tm, tn, kb0, kb1);
       const long gi = (long)tm * C::BM + row;
       const bool row_ok = gi < w.m;
-      const int ei = row_ok ? b200_scale_exp(p.amax[gi]) : 0;
+      const int ei = row_ok ? p.aexp[gi] : 0;
       if (kb0 >= kb1) {  // no update: beta * C
         if (row_ok)
           for (int j = 0; j < C::BN; ++j) {
@@ -750,22 +803,34 @@ __global__ void __launch_bounds__(384, 1)
               tc::tmem_ld16(lane_base + (uint32_t)(ch * 16), r);
               tc::tmem_wait_ld();
               if (!row_ok) continue;
+              // The chunk's loads (workspace, and in the last phase C and the
+              // column scales) are issued before its stores.
+              double wv[16], cv[16];
+              int sc[16];
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
                 const int col = ch * 16 + j;
-                double *wp = W + row + (size_t)col * C::BM;
+                wv[j] = ph > 0 ? W[row + (size_t)col * C::BM] : 0.0;
+                const long gj = (long)tn * C::BN + col;
+                const bool in = last && gj < w.n && b200_rel(w.ji, gj, gi);
+                cv[j] = in && p.beta != 0.0 ? (double)((const TC *)p.c)[gi * p.rs_c + gj * p.cs_c]
+                                            : 0.0;
+                sc[j] = in ? p.bexp[gj] : 0;
+              }
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                const int col = ch * 16 + j;
                 double v = ldexp((double)(int)r[j], -7 * (S + 1 - pl));
-                if (ph > 0) v += *wp;
+                if (ph > 0) v += wv[j];
                 if (!last) {
-                  *wp = v;
+                  W[row + (size_t)col * C::BM] = v;
                   continue;
                 }
                 const long gj = (long)tn * C::BN + col;
                 if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
-                TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
-                double out = p.alpha * ldexp(v, ei + b200_scale_exp(p.bmax[gj]));
-                if (p.beta != 0.0) out = fma(p.beta, (double)*cij, out);
-                *cij = (TC)out;
+                double out = p.alpha * b200_pow2_scale(v, ei + sc[j]);
+                if (p.beta != 0.0) out = fma(p.beta, cv[j], out);
+                ((TC *)p.c)[gi * p.rs_c + gj * p.cs_c] = (TC)out;
               }
             }
           }
@@ -794,6 +859,17 @@ __global__ void __launch_bounds__(384, 1)
 #pragma unroll
           for (int l = 0; l < B200_MAX_MODULI; ++l)
             rv[l] = l < S ? base[(size_t)l * (C::BM * C::BN / 8)] : make_uint2(0, 0);
+          // The chunk's C values and column scales load with the residues,
+          // before any of its stores (one round trip, not one per element).
+          TC cv[8];
+          int sc[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const long gj = (long)tn * C::BN + ch8 * 8 + j;
+            const bool in = gj < w.n && b200_rel(w.ji, gj, gi);
+            cv[j] = in && p.beta != 0.0 ? ((const TC *)p.c)[gi * p.rs_c + gj * p.cs_c] : TC(0);
+            sc[j] = in ? p.bexp[gj] : 0;
+          }
 #pragma unroll
           for (int l = 0; l < B200_MAX_MODULI; ++l) {
             if (l >= S) break;
@@ -810,11 +886,10 @@ __global__ void __launch_bounds__(384, 1)
           for (int j = 0; j < 8; ++j) {
             const long gj = (long)tn * C::BN + ch8 * 8 + j;
             if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
-            TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
             const double cp = oz_crt(k, s0[j], s1[j], s2[j]);
-            double out = p.alpha * ldexp(cp, sh + b200_scale_exp(p.bmax[gj]));
-            if (p.beta != 0.0) out = fma(p.beta, (double)*cij, out);
-            *cij = (TC)out;
+            double out = p.alpha * b200_pow2_scale(cp, sh + sc[j]);
+            if (p.beta != 0.0) out = fma(p.beta, (double)cv[j], out);
+            ((TC *)p.c)[gi * p.rs_c + gj * p.cs_c] = (TC)out;
           }
         }
       }
@@ -904,15 +979,16 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
   // FP64 inputs carry 53 significant bits, FP32 inputs 24: a few bits more
   // than that keeps elements a few binades below the row maximum exact.
   if (mod) B200_TRY(oz2_setup(slices, ktot, F64 ? 56 : 27, &moduli, &p.crt, &pa, &pb));
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const int sms = b200_sm_count();
   const int tiles = (int)((mpad / C::BM) * (npad / C::BN));
   const int grid = tiles < sms ? tiles : sms;
 
   void *ap = nullptr, *bp = nullptr, *amax = nullptr, *bmax = nullptr, *work = nullptr;
-  int st = b200_alloc(&amax, sizeof(unsigned long long) * (mpad + npad));
+  int st = b200_alloc(&amax, (sizeof(unsigned long long) + sizeof(int)) * (mpad + npad));
+  int *exps = nullptr;
   if (st == B200_OK) {
     bmax = (unsigned long long *)amax + mpad;
+    exps = (int *)((unsigned long long *)amax + mpad + npad);
     st = cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * (mpad + npad), s) == cudaSuccess
              ? B200_OK
              : b200_set_error(B200_ECUDA, "memset failed");
@@ -936,6 +1012,7 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
     if (st == B200_OK)
       st = launch_absmax<T>(vb[t], true, d->n, d->k, (unsigned long long *)bmax, s);
   }
+  if (st == B200_OK) st = launch_scale_exps((const unsigned long long *)amax, exps, mpad + npad, s);
   for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
     long kk0 = (long)t * d->k, kk1 = t + 1 == d->npairs ? kpad : kk0 + d->k;
     const int xform = mod ? PACK_INT8_MODULI : PACK_INT8_SLICES;
@@ -971,8 +1048,8 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
     p.rs_c = d->rs_c;
     p.cs_c = d->cs_c;
     p.work = work;
-    p.amax = (const unsigned long long *)amax;
-    p.bmax = (const unsigned long long *)bmax;
+    p.aexp = exps;
+    p.bexp = exps + mpad;
     p.err = b200_device_error_word();
     auto kern = tc_ozaki_kernel<true, T>;
     if constexpr (F64) {

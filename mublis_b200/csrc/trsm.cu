@@ -181,8 +181,13 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   if (rows <= BIG) {
     // X_b = inv(A_bb) B_b in place: the packed path packs B_b before the
     // product writes it.  Plain precision: the diagonal-block solve is FP64
-    // (FP32) whatever form the updates use.
+    // (FP32) whatever form the updates use.  inv(A_bb) is triangular like
+    // A_bb, so it goes in as a triangular operand with the matching k range
+    // per row tile (pi LOWER / UPPER): the zero tiles are not multiplied.
     b200_l3_desc_t g = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
+    g.product.domain.pi = lower ? MUBLIS_L3_LOWER : MUBLIS_L3_UPPER;
+    g.product.a.struc = MUBLIS_STRUC_TRIANGULAR;
+    g.product.a.uplo = d->uplo;
     g.m = (int)rows;
     g.n = d->n;
     g.k = (int)rows;
@@ -206,6 +211,7 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   long t0 = lower ? mid : r0, t1 = lower ? r1 : mid;
   B200_TRY(trsm_rec<T>(d, inv, s0, s1));
   b200_l3_desc_t g = plain_gemm_desc(d->dtype, d->form, d->slices);
+  g.policy_n = d->policy_n;
   g.m = (int)(t1 - t0);
   g.n = d->n;
   g.k = (int)(s1 - s0);

@@ -7,6 +7,7 @@ restatement, or against a double-double evaluation of sampled entries at
   bf16x6 (FP32)         4 * k * 2^-24                  (same as plain)
   bf16x3 (FP32)         2^-15   (16-bit split of each input: ~2^-17 per
                                  element, not k-dependent)
+  fp16x3 (FP32)         4 * k * 2^-24  (scaled fp16 split: ~24-bit inputs)
   ozaki:8 (FP64)        4 * k * 2^-53                  (same as plain)
   ozaki:7 (FP64)        2^-44
   ozaki2 (FP64, 16 moduli, ~55-bit inputs)   4 * k * 2^-53
@@ -32,6 +33,7 @@ pytestmark = pytest.mark.gpu
 TOL = {
     "plain": lambda k, u: 4 * k * u,
     "bf16x6": lambda k, u: 4 * k * 2.0 ** -24,
+    "fp16x3": lambda k, u: 4 * k * 2.0 ** -24,
     "bf16x3": lambda k, u: 2.0 ** -15,
     "ozaki:8": lambda k, u: 4 * k * 2.0 ** -53,
     "ozaki:7": lambda k, u: 2.0 ** -44,
@@ -71,7 +73,7 @@ FAMILY = [("gemm", dict(ta=False, tb=False)), ("gemm", dict(ta=True, tb=True)),
           ("trsm", dict(right=False, lower=True, ta=False, unit=False))]
 
 
-@pytest.mark.parametrize("form", ["bf16x3", "bf16x6", "ozaki2"])
+@pytest.mark.parametrize("form", ["bf16x3", "bf16x6", "fp16x3", "ozaki2"])
 @pytest.mark.parametrize("routine,flags", FAMILY, ids=[f"{r}{i}" for i, (r, _) in enumerate(FAMILY)])
 def test_fp32_tensor_forms(lib, form, routine, flags):
     case = dict(routine=routine, dtype="float32", order="F", m=640, n=544, k=704, alpha=0.75,
@@ -122,6 +124,33 @@ def test_auto_form_fp64_picks_emulation_within_plain_error(lib):
     den = np.linalg.norm(a) * np.linalg.norm(b) + 0.5 * np.linalg.norm(c0)
     err = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
     assert err <= 4 * n * 2.0 ** -53, err
+
+
+def test_auto_form_fp32_large_is_fp16x3_within_plain_error(lib):
+    """From 4096 on "auto" runs FP32 GEMM as fp16x3: the result is
+    bit-identical to an explicit fp16x3 call, and its error against
+    double-double values of 512 sampled entries is within plain's bound."""
+    n = 4096
+    a = orc.fill(n, n, np.float32, 13, 0)
+    b = orc.fill(n, n, np.float32, 13, 1)
+    c0 = orc.fill(n, n, np.float32, 13, 2)
+    rng = np.random.default_rng(5)
+    rows, cols = rng.integers(0, n, 512), rng.integers(0, n, 512)
+    hi, lo = orc.dd_gemm_entries(a, b, rows, cols, alpha=1.0, beta=0.5, c0=c0)
+    out = {}
+    for form in ("auto", "fp16x3"):
+        assert lib.mublis_b200_set_form(b"s", form.encode()) == 0
+        c = c0.copy(order="F")
+        assert lib.mublis_sgemm(0, 0, n, n, n, 1.0, a.ctypes.data, 1, n, b.ctypes.data, 1, n,
+                                0.5, c.ctypes.data, 1, n) == 0, mb.last_error(lib)
+        out[form] = c
+    lib.mublis_b200_set_form(b"s", b"plain")
+    np.testing.assert_array_equal(out["auto"], out["fp16x3"])
+    d = out["auto"][rows, cols].astype(np.float64) - (hi + lo)
+    den = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64)) + \
+        0.5 * np.linalg.norm(c0.astype(np.float64))
+    err = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
+    assert err <= 4 * n * 2.0 ** -24, err
 
 
 def test_wide_range_inputs_ozaki(lib):
@@ -203,7 +232,7 @@ def test_precision_study_8192(lib, kind):
     rows, cols = _full_lines(n, 256, 7)
     ns = len(rows)
     table = {}
-    for p, forms in (("s", ["plain", "bf16x3", "bf16x6", "ozaki2"]),
+    for p, forms in (("s", ["plain", "bf16x3", "bf16x6", "fp16x3", "ozaki2"]),
                      ("d", ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
         a, b, c0 = (_device_matrix(torch, lib, p, n, 0, i, kind) for i in range(3))
         # torch holds the column-major matrices transposed: a.cpu() is A^T in
@@ -239,6 +268,7 @@ def test_precision_study_8192(lib, kind):
     assert table["dgemm ozaki:8"][0] <= table["dgemm plain"][0]
     assert table["dgemm ozaki2"][0] <= table["dgemm plain"][0]
     assert table["sgemm ozaki2"][0] <= table["sgemm plain"][0]
+    assert table["sgemm fp16x3"][0] <= 1.5 * table["sgemm plain"][0]
     assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
     assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)
 
