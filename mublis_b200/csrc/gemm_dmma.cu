@@ -82,31 +82,6 @@ __device__ __forceinline__ bool tile_krange(const DmmaGemmArgs &p, int tm, int t
   return true;
 }
 
-// L2 prefetch of the C tile the epilogue reads (beta != 0), issued a few
-// k-blocks before the tile's last: the epilogue's per-element load / store
-// pairs then wait on L2 rather than HBM.  Unit-stride C only (other layouts
-// skip it); each of the 256 consumer threads covers half a column (or row)
-// of the 128 x 128 tile, 64 elements, one 128-byte line at a time, and only
-// addresses inside the m x n matrix are touched.
-__device__ __forceinline__ void prefetch_c_tile(const DmmaGemmArgs &p, int tm, int tn, int tid) {
-  const long m0 = (long)tm * BM, n0 = (long)tn * BN;
-  long slow, fast0, slow_len, fast_len, slow_stride;
-  if (p.rs_c == 1) {
-    slow = n0 + (tid >> 1), fast0 = m0 + (tid & 1) * 64;
-    slow_len = p.n, fast_len = p.m, slow_stride = p.cs_c;
-  } else if (p.cs_c == 1) {
-    slow = m0 + (tid >> 1), fast0 = n0 + (tid & 1) * 64;
-    slow_len = p.m, fast_len = p.n, slow_stride = p.rs_c;
-  } else {
-    return;
-  }
-  if (slow >= slow_len) return;
-  const double *line = p.c + slow * slow_stride;
-#pragma unroll
-  for (int q = 0; q < 64; q += 16)
-    if (fast0 + q < fast_len) asm volatile("prefetch.global.L2 [%0];" ::"l"(line + fast0 + q));
-}
-
 __global__ void __launch_bounds__(THREADS, 1)
     dmma_gemm_kernel(const __grid_constant__ DmmaGemmArgs p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -172,10 +147,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
-    // C prefetch distance: a few k-blocks before the epilogue reads C.
-    const int kt_pf = kt1 - 4 > kt0 ? kt1 - 4 : kt0;
     for (int kt = kt0; kt < kt1; ++kt) {
-      if (kt == kt_pf && p.beta != 0.0) prefetch_c_tile(p, tm, tn, threadIdx.x);
       const int wok = tc::mbar_wait(&full[stage], phase, abort_flag, p.err);
       if (!__all_sync(0xffffffffu, wok)) return;
       const double2 *As = (const double2 *)(smem + stage * STAGE_BYTES) + wm * 4 * 32 + lane;

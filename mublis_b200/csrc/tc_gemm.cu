@@ -157,6 +157,17 @@ struct Bf16Cfg {
   static constexpr uint32_t TMEM_COLS = 512;
 };
 
+// Register split of the BF16 / FP16 kernel: launched at 168 registers per
+// thread (384 threads), warpgroup 0 (TMA producer, MMA issuer, TMEM owner)
+// drops to 48 and the two epilogue warpgroups rise to 224, which holds the
+// 128 FP32 running sums per thread, four 16-column TMEM loads in flight and
+// a 16-column batch of C without spilling (at one 168 budget for all
+// warps, the fp16x3 epilogue spilled part of its running sums to local
+// memory on every window drain).
+constexpr int BF16_LAUNCH_REGS = 168, BF16_PRODUCER_REGS = 48, BF16_EPILOGUE_REGS = 224;
+static_assert(128 * BF16_PRODUCER_REGS + 256 * BF16_EPILOGUE_REGS <= 384 * BF16_LAUNCH_REGS,
+              "register split exceeds the launch allocation");
+
 template <int TERMS, int STAGES, bool F16 = false>
 __global__ void __launch_bounds__(384, 1)
     tc_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -202,6 +213,10 @@ __global__ void __launch_bounds__(384, 1)
     return smem + s * C::STAGE_BYTES + TERMS * C::A_TILE + t * C::B_TILE;
   };
 
+  // Each warpgroup's register share is set at the top of the branch that
+  // holds its role, so the compiler allocates each role's code against it.
+  if (warp < 4) {
+  tc::setmaxnreg_dec<BF16_PRODUCER_REGS>();
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int stage = 0;
@@ -282,7 +297,9 @@ __global__ void __launch_bounds__(384, 1)
       tc::mma_commit(drain);
       tc::mbar_wait(drain, 0, abort_flag, p.err);
     }
-  } else if (warp >= 4) {
+  }
+  } else {
+    tc::setmaxnreg_inc<BF16_EPILOGUE_REGS>();
     // ---------------- epilogue ----------------
     const int quad = warp & 3;        // TMEM lanes 32*quad .. 32*quad+31
     const int half = (warp - 4) >> 2; // columns [half*128, half*128+128)
@@ -311,22 +328,39 @@ __global__ void __launch_bounds__(384, 1)
         continue;
       }
       const int nwin = (kb1 - kb0 + C::FLUSH - 1) / C::FLUSH;
+      float *crow = p.c + gi * p.rs_c;
       for (int win = 0; win < nwin; ++win) {
+        if (win == nwin - 1 && row_ok && p.beta != 0.f) {
+          // While the tile's last window is multiplied, pull the C values
+          // the final store reads into L2.
+#pragma unroll 8
+          for (int j = 0; j < C::HALF; ++j)
+            if (gj0 + j < w.n)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + (gj0 + j) * p.cs_c));
+        }
         // Every lane observes the barrier; the outcome is made warp-uniform
         // because the TMEM loads below are .sync.aligned.
         int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
         if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
         tc::tc_fence_after();
         const uint32_t base = lane_base + (uint32_t)(acc * C::BN + half * C::HALF);
+        // Four 16-column TMEM loads in flight per wait.
 #pragma unroll
-        for (int g = 0; g < C::HALF / 16; ++g) {
-          uint32_t r[16];
-          tc::tmem_ld16(base + (uint32_t)(g * 16), r);
+        for (int g0 = 0; g0 < C::HALF / 16; g0 += 4) {
+          uint32_t r[4][16];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tc::tmem_ld16(base + (uint32_t)((g0 + q) * 16), r[q]);
           tc::tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            run[g * 16 + j] = win == 0 ? __uint_as_float(r[j])
-                                       : __fadd_rn(run[g * 16 + j], __uint_as_float(r[j]));
+          for (int q = 0; q < 4; ++q) tc::tmem_tie16(r[q]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int c = (g0 + q) * 16 + j;
+              run[c] = win == 0 ? __uint_as_float(r[q][j])
+                                : __fadd_rn(run[c], __uint_as_float(r[q][j]));
+            }
         }
         tc::tc_fence_before();
         tc::mbar_arrive(&tempty[acc]);
@@ -339,7 +373,6 @@ __global__ void __launch_bounds__(384, 1)
         // chain per element pays one memory round trip each, and while this
         // store runs the MMAs of the next tile stall after two windows.
         const int ei = F16 ? p.aexp[gi] : 0;
-        float *crow = p.c + gi * p.rs_c;
 #pragma unroll
         for (int j0 = 0; j0 < C::HALF; j0 += 16) {
           float cv[16];
@@ -382,6 +415,13 @@ int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &
   static bool configured = false;
   if (!configured) {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    // The warpgroup register split assumes this launch allocation; with
+    // fewer registers per thread the epilogue's increase could never be
+    // granted, so refuse to launch rather than wait.
+    cudaFuncAttributes fa;
+    B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (fa.numRegs != BF16_LAUNCH_REGS || C::THREADS != 384)
+      return b200_set_error(B200_EINVAL, "bf16 kernel: unexpected register allocation");
     configured = true;
   }
   const int sms = b200_sm_count();

@@ -15,8 +15,8 @@ restatement, or against a double-double evaluation of sampled entries at
   ozaki2:14 (FP64, ~49-bit inputs at k=700)  2^-44
   ozaki2:6 (FP64, ~18-bit inputs: checks the CRT with M < 2^84)  2^-14
 The 8192^3 study also checks the headline claims: bf16x6 has the error of
-plain FP32 (within 1.5x), and ozaki:8 and ozaki2 have at most the error of
-plain FP64.
+plain FP32 (within 1.5x), fp16x3 at most plain FP32's, and ozaki:8 and
+ozaki2 at most the error of plain FP64.
 Run with -s to print the measured table.
 """
 import ctypes
@@ -268,7 +268,7 @@ def test_precision_study_8192(lib, kind):
     assert table["dgemm ozaki:8"][0] <= table["dgemm plain"][0]
     assert table["dgemm ozaki2"][0] <= table["dgemm plain"][0]
     assert table["sgemm ozaki2"][0] <= table["sgemm plain"][0]
-    assert table["sgemm fp16x3"][0] <= 1.5 * table["sgemm plain"][0]
+    assert table["sgemm fp16x3"][0] <= table["sgemm plain"][0]
     assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
     assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)
 
