@@ -157,16 +157,23 @@ struct Bf16Cfg {
   static constexpr uint32_t TMEM_COLS = 512;
 };
 
-// Register split of the BF16 / FP16 kernel: launched at 168 registers per
+// Register split of the tensor-core kernels: launched at 168 registers per
 // thread (384 threads), warpgroup 0 (TMA producer, MMA issuer, TMEM owner)
-// drops to 48 and the two epilogue warpgroups rise to 224, which holds the
+// drops to 56 and the two epilogue warpgroups rise to 216, which holds the
 // 128 FP32 running sums per thread, four 16-column TMEM loads in flight and
 // a 16-column batch of C without spilling (at one 168 budget for all
 // warps, the fp16x3 epilogue spilled part of its running sums to local
 // memory on every window drain).
-constexpr int BF16_LAUNCH_REGS = 168, BF16_PRODUCER_REGS = 48, BF16_EPILOGUE_REGS = 224;
-static_assert(128 * BF16_PRODUCER_REGS + 256 * BF16_EPILOGUE_REGS <= 384 * BF16_LAUNCH_REGS,
-              "register split exceeds the launch allocation");
+constexpr int TC_PRODUCER_REGS = 56, TC_EPILOGUE_REGS = 216;
+
+// True when warpgroup 0 dropping to TC_PRODUCER_REGS frees enough for the
+// two epilogue warpgroups to rise to TC_EPILOGUE_REGS from the compiled
+// kernel's per-thread allocation `launch_regs` (384 threads).  An increase
+// that cannot be granted waits forever, so the launchers check this first.
+inline bool tc_register_split_fits(int launch_regs) {
+  return launch_regs >= TC_PRODUCER_REGS &&
+         128L * (launch_regs - TC_PRODUCER_REGS) >= 256L * (TC_EPILOGUE_REGS - launch_regs);
+}
 
 template <int TERMS, int STAGES, bool F16 = false>
 __global__ void __launch_bounds__(384, 1)
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(384, 1)
   // Each warpgroup's register share is set at the top of the branch that
   // holds its role, so the compiler allocates each role's code against it.
   if (warp < 4) {
-  tc::setmaxnreg_dec<BF16_PRODUCER_REGS>();
+  tc::setmaxnreg_dec<TC_PRODUCER_REGS>();
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int stage = 0;
@@ -299,7 +306,7 @@ __global__ void __launch_bounds__(384, 1)
     }
   }
   } else {
-    tc::setmaxnreg_inc<BF16_EPILOGUE_REGS>();
+    tc::setmaxnreg_inc<TC_EPILOGUE_REGS>();
     // ---------------- epilogue ----------------
     const int quad = warp & 3;        // TMEM lanes 32*quad .. 32*quad+31
     const int half = (warp - 4) >> 2; // columns [half*128, half*128+128)
@@ -420,8 +427,8 @@ int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &
     // granted, so refuse to launch rather than wait.
     cudaFuncAttributes fa;
     B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
-    if (fa.numRegs != BF16_LAUNCH_REGS || C::THREADS != 384)
-      return b200_set_error(B200_EINVAL, "bf16 kernel: unexpected register allocation");
+    if (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
+      return b200_set_error(B200_EINVAL, "bf16 kernel: register split does not fit its launch");
     configured = true;
   }
   const int sms = b200_sm_count();
@@ -684,6 +691,10 @@ __global__ void __launch_bounds__(384, 1)
   auto sa = [&](int st) { return smem + st * C::STAGE_BYTES; };
   auto sb = [&](int st) { return smem + st * C::STAGE_BYTES + C::A_TILE; };
 
+  // Register shares per warpgroup, set where each role begins (as in the
+  // BF16 kernel): the epilogue keeps four 16-column TMEM loads in flight.
+  if (warp < 4) {
+  tc::setmaxnreg_dec<TC_PRODUCER_REGS>();
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer ----------------
     int stage = 0, issued = 0;
@@ -769,7 +780,9 @@ __global__ void __launch_bounds__(384, 1)
       tc::mma_commit(drain);
       tc::mbar_wait(drain, 0, abort_flag, p.err);
     }
-  } else if (warp >= 4) {
+  }
+  } else {
+    tc::setmaxnreg_inc<TC_EPILOGUE_REGS>();
     // ---------------- epilogue ----------------
     // Warps 4-7 drain the accumulator of rows 0-127, warps 8-11 the one of
     // rows 128-255; each warp reads the TMEM lanes of its quadrant.
@@ -814,27 +827,36 @@ __global__ void __launch_bounds__(384, 1)
             const int m = p.crt.m[pl], bias = p.crt.bias[pl];
             const unsigned mg = p.crt.mg[pl];
             uint4 *Rl = (uint4 *)(R + (size_t)pl * C::BM * C::BN) + row;
-            // The next chunk's TMEM load is in flight while this one is reduced.
-            uint32_t rb[2][16];
-            tc::tmem_ld16(lane_base, rb[0]);
-            tc::tmem_wait_ld_dep(rb[0]);
+            // Four 16-column TMEM loads in flight per wait: one round trip
+            // per 64 columns instead of one per 16.
 #pragma unroll
-            for (int ch = 0; ch < C::BN / 16; ++ch) {
-              if (ch + 1 < C::BN / 16)
-                tc::tmem_ld16(lane_base + (uint32_t)((ch + 1) * 16), rb[(ch + 1) & 1]);
-              const uint4 prev = cc > 0 ? Rl[ch * C::BM] : make_uint4(0, 0, 0, 0);
-              uint32_t out[4] = {0, 0, 0, 0};
+            for (int ch0 = 0; ch0 < C::BN / 16; ch0 += 4) {
+              uint32_t rb[4][16];
 #pragma unroll
-              for (int j = 0; j < 16; ++j) {
-                int res = b200_sym_mod((int)rb[ch & 1][j], m, mg, bias);  // |C'_l| <= 2^29
-                if (cc > 0) {
-                  const uint32_t word = j < 4 ? prev.x : j < 8 ? prev.y : j < 12 ? prev.z : prev.w;
-                  res = b200_sym_mod(res + (int)(int8_t)(word >> (8 * (j & 3))), m, mg, bias);
+              for (int q = 0; q < 4; ++q)
+                tc::tmem_ld16(lane_base + (uint32_t)((ch0 + q) * 16), rb[q]);
+              uint4 prev[4];
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                prev[q] = cc > 0 ? Rl[(ch0 + q) * C::BM] : make_uint4(0, 0, 0, 0);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int q = 0; q < 4; ++q) tc::tmem_tie16(rb[q]);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                uint32_t out[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  int res = b200_sym_mod((int)rb[q][j], m, mg, bias);  // |C'_l| <= 2^29
+                  if (cc > 0) {
+                    const uint4 pv = prev[q];
+                    const uint32_t word = j < 4 ? pv.x : j < 8 ? pv.y : j < 12 ? pv.z : pv.w;
+                    res = b200_sym_mod(res + (int)(int8_t)(word >> (8 * (j & 3))), m, mg, bias);
+                  }
+                  out[j >> 2] |= (uint32_t)(res & 0xff) << (8 * (j & 3));
                 }
-                out[j >> 2] |= (uint32_t)(res & 0xff) << (8 * (j & 3));
+                Rl[(ch0 + q) * C::BM] = make_uint4(out[0], out[1], out[2], out[3]);
               }
-              Rl[ch * C::BM] = make_uint4(out[0], out[1], out[2], out[3]);
-              if (ch + 1 < C::BN / 16) tc::tmem_wait_ld_dep(rb[(ch + 1) & 1]);
             }
           } else {
 #pragma unroll 1
@@ -1100,6 +1122,13 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) !=
           cudaSuccess)
         st = b200_set_error(B200_ECUDA, "ozaki: smem attribute");
+      // The warpgroup register split must fit the compiled allocation (an
+      // increase that cannot be granted would wait forever).
+      cudaFuncAttributes fa;
+      if (st == B200_OK && cudaFuncGetAttributes(&fa, kern) != cudaSuccess)
+        st = b200_set_error(B200_ECUDA, "ozaki: function attributes");
+      if (st == B200_OK && (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs)))
+        st = b200_set_error(B200_EINVAL, "ozaki kernel: register split does not fit its launch");
       configured[mod] = st == B200_OK;
     }
     if (st == B200_OK) {
