@@ -640,6 +640,22 @@ extern "C" int b200_l3_is_plain_gemm(const b200_l3_desc_t *d) {
          p.b.struc == MUBLIS_STRUC_GENERAL;
 }
 
+// Without a tuned choice: the class's default tile, stepped down to smaller
+// tiles while the group would leave more than half of the SMs without a
+// tile (a few 512 x 512 products, as TRSM's inverse doubling issues, are 16
+// tiles each at 128 x 128).
+int fill_variant(const std::vector<GemmEntry> &es, int v) {
+  static const int smaller[TILE_VARIANTS] = {-1, TILE_32, TILE_64, TILE_128x64};
+  auto tiles = [&](int var) {
+    long t = 0;
+    for (const auto &e : es)
+      t += b200_ceil_div(e.m, kTileBM[var]) * b200_ceil_div(e.n, kTileBN[var]);
+    return t;
+  };
+  while (smaller[v] >= 0 && 2 * tiles(v) < sm_count()) v = smaller[v];
+  return v;
+}
+
 extern "C" int b200_grouped_gemm_async(int dtype, const b200_l3_desc_t *const *descs, int count,
                                        void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
@@ -673,11 +689,13 @@ extern "C" int b200_grouped_gemm_async(int dtype, const b200_l3_desc_t *const *d
     if (cls[c].empty()) continue;
     int bucket = 31 - __builtin_clz((unsigned)cls[c].size());
     int v;
+    bool tuned;
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
-      v = g_tuned[dtype == B200_F64][c][bucket] ? g_tuned[dtype == B200_F64][c][bucket] - 1
-                                                : kDefaultVariant[c];
+      tuned = g_tuned[dtype == B200_F64][c][bucket] != 0;
+      v = tuned ? g_tuned[dtype == B200_F64][c][bucket] - 1 : kDefaultVariant[c];
     }
+    if (!tuned) v = fill_variant(cls[c], v);
     g[c].entries = cls[c];
     g[c].variant = v;
     int t = 0;

@@ -8,17 +8,19 @@
 //   * recursive halving: solve the top half, update the bottom half with one
 //     GEMM (k = half the order, so it runs at GEMM speed), solve the bottom
 //     half (upper: mirror image);
-//   * leaves are the 512 x 512 diagonal blocks, inverted up front: one launch
-//     inverts every 64 x 64 diagonal block by substitution against the
-//     reciprocal diagonal (computed once and multiplied -- never divided --
-//     as the reference does), then three doubling steps of two batched
-//     (grouped) GEMM launches each build the 128-, 256- and 512-blocks,
+//   * leaves are the 512 x 512 (1024 x 1024 for large solves) diagonal
+//     blocks, inverted up front: one launch inverts every 64 x 64 diagonal
+//     block by substitution against the reciprocal diagonal (computed once
+//     and multiplied -- never divided -- as the reference does), then
+//     doubling steps of two batched (grouped) GEMM launches each build the
+//     128-, 256-, 512- (and 1024-) blocks,
 //     inv([A11 0; A21 A22]) = [inv11 0; -inv22 A21 inv11  inv22];
-//   * each leaf solve is then X_b = inv(A_bb) B_b, one 512-deep GEMM over all
-//     right-hand sides (plain FP64/FP32: the diagonal blocks never use an
-//     emulated form), and every update is a GEMM of k >= 512 on the packed
-//     path (and the caller's form).  512-row leaves give those GEMMs at least
-//     128 output tiles of 128 x 128 for 148 SMs (256-row leaves gave 64);
+//   * each leaf solve is then X_b = inv(A_bb) B_b, one triangular product
+//     over all right-hand sides (plain FP64/FP32: the diagonal blocks never
+//     use an emulated form), and every update is a GEMM of k >= 512 on the
+//     packed path (and the caller's form).  512-row leaves give those GEMMs
+//     at least 128 output tiles of 128 x 128 for 148 SMs (256-row leaves
+//     gave 64);
 //   * the unit diagonal and the unstored triangle are never read.
 // alpha is applied once up front (the reference's alpha_eff on the first
 // block, trsm.c:96-97).
@@ -31,19 +33,27 @@
 namespace {
 
 constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
-constexpr int BIG = 512;  // inverted diagonal blocks the solve uses (leaves)
-constexpr int PER_BIG = BIG / LEAF;
+
+// Order of the inverted diagonal blocks the solve uses (its leaves): 512, or
+// 1024 for large solves.  A leaf product inv(A_bb) B_b over n right-hand
+// sides is a triangular GEMM of 512 (1024) rows: 1024-row leaves give it
+// 256 output tiles of 128 x 128 instead of 128 (148 SMs) and remove the
+// level of 512-row updates below them, for one more doubling step (about
+// m * 512^2 extra flops).  With few right-hand sides that doubling step
+// would cost more than it saves, so 1024 is used only from m >= 4096 and
+// n >= 2048.
+int leaf_order(long m, long n) { return m >= 4096 && n >= 2048 ? 1024 : 512; }
 
 // One CTA per LEAF block: thread j computes column j of the inverse of the
 // block's (lower or upper) triangle by substitution, L x = e_j.  Rows past
 // the matrix order are padded with the identity.  Output: big block
-// b / PER_BIG is a BIG x BIG column-major matrix at inv + (b / PER_BIG) *
-// BIG * BIG (zeroed beforehand); LEAF block b lands on its diagonal at
-// offset (b % PER_BIG) * LEAF.
+// b / per_big (per_big = big / LEAF) is a big x big column-major matrix at
+// inv + (b / per_big) * big * big (zeroed beforehand); LEAF block b lands on
+// its diagonal at offset (b % per_big) * LEAF.
 template <typename T>
 __global__ void __launch_bounds__(LEAF) trsm_inv_diag_kernel(int m, const T *a, long rs_a,
                                                               long cs_a, bool lower, bool unit,
-                                                              T *inv) {
+                                                              T *inv, int big) {
   __shared__ T L[LEAF][LEAF + 1];
   const int b = blockIdx.x, j = threadIdx.x;
   const long r0 = (long)b * LEAF;
@@ -81,18 +91,19 @@ __global__ void __launch_bounds__(LEAF) trsm_inv_diag_kernel(int m, const T *a, 
       x[i] = r * L[i][i];
     }
   }
-  const size_t off = (size_t)(b % PER_BIG) * LEAF;
-  T *out = inv + (size_t)(b / PER_BIG) * BIG * BIG + off * (BIG + 1) + (size_t)j * BIG;
+  const int per_big = big / LEAF;
+  const size_t off = (size_t)(b % per_big) * LEAF;
+  T *out = inv + (size_t)(b / per_big) * big * big + off * (big + 1) + (size_t)j * big;
 #pragma unroll
   for (int i = 0; i < LEAF; ++i) out[i] = x[i];
 }
 
 template <typename T>
 int launch_inv_diag(int m, const T *a, long rs_a, long cs_a, bool lower, bool unit, T *inv,
-                    cudaStream_t s) {
+                    int big, cudaStream_t s) {
   const int blocks = (int)b200_ceil_div(m, LEAF);
   B200ProfScope prof(sizeof(T) == 4 ? "trsm_inv_s" : "trsm_inv_d", s);
-  trsm_inv_diag_kernel<T><<<blocks, LEAF, 0, s>>>(m, a, rs_a, cs_a, lower, unit, inv);
+  trsm_inv_diag_kernel<T><<<blocks, LEAF, 0, s>>>(m, a, rs_a, cs_a, lower, unit, inv, big);
   B200_LAUNCH_CHECK();
   return B200_OK;
 }
@@ -122,17 +133,17 @@ b200_l3_desc_t plain_gemm_desc(int dtype, int form, int slices) {
 // pair whose second half is cut by the matrix order uses only its valid
 // m2 rows/columns; the identity padding makes the rest already correct.
 template <typename T>
-int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, cudaStream_t s) {
+int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, const long big, cudaStream_t s) {
   const T *a = (const T *)d->a;
   const bool lower = d->uplo == MUBLIS_LOWER;
   const long m = d->m;
-  for (long h = LEAF; h < BIG; h *= 2) {
+  for (long h = LEAF; h < big; h *= 2) {
     std::vector<b200_l3_desc_t> g1, g2;
     for (long r0 = 0; r0 + h < m; r0 += 2 * h) {
       const int m2 = (int)std::min(h, m - r0 - h);
-      T *blk = inv + (r0 / BIG) * BIG * BIG;
-      const long o1 = r0 % BIG, o2 = o1 + h;
-      const T *inv11 = blk + o1 * (BIG + 1), *inv22 = blk + o2 * (BIG + 1);
+      T *blk = inv + (r0 / big) * big * big;
+      const long o1 = r0 % big, o2 = o1 + h;
+      const T *inv11 = blk + o1 * (big + 1), *inv22 = blk + o2 * (big + 1);
       T *t = tmp + (r0 / (2 * h)) * h * h;
       b200_l3_desc_t p = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
       b200_l3_desc_t q = p;
@@ -142,21 +153,21 @@ int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, cudaStream_t s) {
       if (lower) {  // T (m2 x h) = A21 inv11;  X21 = -inv22[m2 x m2] T
         p.m = m2, p.n = (int)h, p.k = (int)h;
         p.a[0] = a + (r0 + h) * d->rs_a + r0 * d->cs_a, p.rs_a[0] = d->rs_a, p.cs_a[0] = d->cs_a;
-        p.b[0] = inv11, p.rs_b[0] = 1, p.cs_b[0] = BIG;
+        p.b[0] = inv11, p.rs_b[0] = 1, p.cs_b[0] = big;
         q.m = m2, q.n = (int)h, q.k = m2;
-        q.a[0] = inv22, q.rs_a[0] = 1, q.cs_a[0] = BIG;
-        q.c = blk + o2 + o1 * BIG;
+        q.a[0] = inv22, q.rs_a[0] = 1, q.cs_a[0] = big;
+        q.c = blk + o2 + o1 * big;
       } else {  // T (h x m2) = A12 inv22[m2 x m2];  X12 = -inv11 T
         p.m = (int)h, p.n = m2, p.k = m2;
         p.a[0] = a + r0 * d->rs_a + (r0 + h) * d->cs_a, p.rs_a[0] = d->rs_a, p.cs_a[0] = d->cs_a;
-        p.b[0] = inv22, p.rs_b[0] = 1, p.cs_b[0] = BIG;
+        p.b[0] = inv22, p.rs_b[0] = 1, p.cs_b[0] = big;
         q.m = (int)h, q.n = m2, q.k = (int)h;
-        q.a[0] = inv11, q.rs_a[0] = 1, q.cs_a[0] = BIG;
-        q.c = blk + o1 + o2 * BIG;
+        q.a[0] = inv11, q.rs_a[0] = 1, q.cs_a[0] = big;
+        q.c = blk + o1 + o2 * big;
       }
       p.c = t, p.rs_c = 1, p.cs_c = h;
       q.b[0] = t, q.rs_b[0] = 1, q.cs_b[0] = h;
-      q.rs_c = 1, q.cs_c = BIG;
+      q.rs_c = 1, q.cs_c = big;
       g1.push_back(p);
       g2.push_back(q);
     }
@@ -173,12 +184,12 @@ int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, cudaStream_t s) {
 }
 
 template <typename T>
-int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
+int trsm_rec(const b200_trsm_desc_t *d, const T *inv, const long big, long r0, long r1) {
   const T *a = (const T *)d->a;
   T *b = (T *)d->b;
   const bool lower = d->uplo == MUBLIS_LOWER;
   long rows = r1 - r0;
-  if (rows <= BIG) {
+  if (rows <= big) {
     // X_b = inv(A_bb) B_b in place: the packed path packs B_b before the
     // product writes it.  Plain precision: the diagonal-block solve is FP64
     // (FP32) whatever form the updates use.  inv(A_bb) is triangular like
@@ -193,9 +204,9 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
     g.k = (int)rows;
     g.alpha = 1.0;
     g.beta = 0.0;
-    g.a[0] = inv + (r0 / BIG) * BIG * BIG;
+    g.a[0] = inv + (r0 / big) * big * big;
     g.rs_a[0] = 1;
-    g.cs_a[0] = BIG;
+    g.cs_a[0] = big;
     g.b[0] = b + r0 * d->rs_b;
     g.rs_b[0] = d->rs_b;
     g.cs_b[0] = d->cs_b;
@@ -204,12 +215,12 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
     g.cs_c = d->cs_b;
     return b200_l3_run(&g);
   }
-  long half = b200_round_up((rows + 1) / 2, BIG);
+  long half = b200_round_up((rows + 1) / 2, big);
   long mid = r0 + half;
   // Rows solved first (src) and rows updated by them (dst).
   long s0 = lower ? r0 : mid, s1 = lower ? mid : r1;
   long t0 = lower ? mid : r0, t1 = lower ? r1 : mid;
-  B200_TRY(trsm_rec<T>(d, inv, s0, s1));
+  B200_TRY(trsm_rec<T>(d, inv, big, s0, s1));
   b200_l3_desc_t g = plain_gemm_desc(d->dtype, d->form, d->slices);
   g.policy_n = d->policy_n;
   g.m = (int)(t1 - t0);
@@ -227,23 +238,24 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, long r0, long r1) {
   g.rs_c = d->rs_b;
   g.cs_c = d->cs_b;
   B200_TRY(b200_l3_run(&g));
-  return trsm_rec<T>(d, inv, t0, t1);
+  return trsm_rec<T>(d, inv, big, t0, t1);
 }
 
 template <typename T>
 int trsm_solve(const b200_trsm_desc_t *d) {
   cudaStream_t s = b200_cur_stream();
   T *inv = nullptr, *tmp = nullptr;
-  const long bigs = b200_ceil_div(d->m, BIG);
-  B200_TRY(b200_alloc((void **)&inv, sizeof(T) * bigs * BIG * BIG));
-  int st = b200_alloc((void **)&tmp, sizeof(T) * bigs * BIG * BIG / 2);
-  if (st == B200_OK && cudaMemsetAsync(inv, 0, sizeof(T) * bigs * BIG * BIG, s) != cudaSuccess)
+  const long big = leaf_order(d->m, d->policy_n > 0 ? d->policy_n : d->n);
+  const long bigs = b200_ceil_div(d->m, big);
+  B200_TRY(b200_alloc((void **)&inv, sizeof(T) * bigs * big * big));
+  int st = b200_alloc((void **)&tmp, sizeof(T) * bigs * big * big / 2);
+  if (st == B200_OK && cudaMemsetAsync(inv, 0, sizeof(T) * bigs * big * big, s) != cudaSuccess)
     st = b200_set_error(B200_ECUDA, "trsm: memset failed");
   if (st == B200_OK)
     st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
-                            d->unit_diag != 0, inv, s);
-  if (st == B200_OK) st = grow_inverse<T>(d, inv, tmp, s);
-  if (st == B200_OK) st = trsm_rec<T>(d, inv, 0, d->m);
+                            d->unit_diag != 0, inv, (int)big, s);
+  if (st == B200_OK) st = grow_inverse<T>(d, inv, tmp, big, s);
+  if (st == B200_OK) st = trsm_rec<T>(d, inv, big, 0, d->m);
   b200_free(tmp);
   b200_free(inv);
   return st;

@@ -343,3 +343,39 @@ def test_context_micro_kernels(lib, p):
         np.testing.assert_allclose(c11, X, rtol=1e-3 if p == "s" else 1e-11,
                                    atol=1e-4 if p == "s" else 1e-12)
         np.testing.assert_array_equal(b11p, c11)
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+@pytest.mark.parametrize("uplo", [1, 2], ids=["lower", "upper"])
+def test_trsm_large_solve_with_1024_leaves(lib, dtype, uplo):
+    """m = n = 4096 TRSM, the size from which the solve inverts 1024 x 1024
+    diagonal blocks (one more doubling step) instead of 512 x 512.  12
+    seeded columns of X against the long-double oracle solve of the same
+    columns (relative forward error <= 4 * m * u on these well-conditioned
+    systems), through device pointers; the same call through host pointers
+    (column panels, each carrying the whole call's n) must be bit-identical."""
+    torch = pytest.importorskip("torch")
+    n, ncheck = 4096, 12
+    dt = np.dtype(dtype)
+    p = "s" if dt == np.float32 else "d"
+    u = 2.0 ** -24 if p == "s" else 2.0 ** -53
+    a = orc.trsm_matrix(n, dt, 5, 0)
+    b = orc.fill(n, n, dt, 5, 1)
+    sel = np.sort(np.random.default_rng(12).choice(n, ncheck, replace=False))
+    ref = np.asfortranarray(b[:, sel])
+    assert getattr(orc.restated(), f"oracle_{p}trsm")(0, uplo, 0, 0, n, ncheck, 1.0,
+                                                     a.ctypes.data, 1, n, ref.ctypes.data, 1,
+                                                     n) == 0
+    fn = getattr(lib, f"mublis_{p}trsm")
+    ad = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    x = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    assert fn(0, uplo, 0, 0, n, n, 1.0, ad.data_ptr(), 1, n, x.data_ptr(), 1, n) == 0, \
+        mb.last_error(lib)
+    dev = np.asfortranarray(x.cpu().numpy().T)
+    got = dev[:, sel].astype(np.float64)
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err <= 4 * n * u, err
+    host = np.asfortranarray(b.copy())
+    assert fn(0, uplo, 0, 0, n, n, 1.0, a.ctypes.data, 1, n, host.ctypes.data, 1, n) == 0, \
+        mb.last_error(lib)
+    np.testing.assert_array_equal(host, dev)
