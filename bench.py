@@ -733,11 +733,16 @@ def main():
         try:
             threads = host_threads()
             r = ref_bench(2048, threads, 1, 0)
+            r1 = ref_bench(2048, 1, 1, 0)  # one call at a time on one core
             cpu = {"value": round(r["gflops_aggregate"] / 1e3, 4), "unit": "TFLOP/s",
                    "cores": threads, "kind": "reference",
                    "sample": f"the 18-call family at m=n=k=2048, one pass per host thread, "
                              f"{threads} threads concurrently, reference linux_avx2 build "
-                             f"(oracle/_ref), wall {r['wall_s']:.1f} s"}
+                             f"(oracle/_ref), wall {r['wall_s']:.1f} s",
+                   "one_thread": {"value": round(r1["gflops_aggregate"] / 1e3, 4),
+                                  "unit": "TFLOP/s", "cores": 1,
+                                  "sample": f"the same family, one pass on one thread, "
+                                            f"wall {r1['wall_s']:.1f} s"}}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unavailable": str(e)}
 
