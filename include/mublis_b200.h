@@ -135,7 +135,10 @@ int mublis_b200_tune_reset(void);
  * TRSMs (order <= 256) waiting together into one grouped launch per
  * precision, and issues the rest asynchronously on a pool of streams,
  * admitting each when its scratch estimate fits the HBM budget.  Calls with
- * host operands keep the direct path. */
+ * host operands keep the direct path.  Creation reserves half the budget
+ * (at most half of the free device memory) in CUDA's stream-ordered pool,
+ * which keeps it for the process, so that requests never wait for the pool
+ * to grow. */
 typedef struct {
   size_t hbm_budget_bytes; /* device memory for handles + scratch (0: 64 GiB) */
   int streams;             /* concurrent streams (0: 4) */

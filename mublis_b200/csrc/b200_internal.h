@@ -94,6 +94,12 @@ int b200_device_count(void);
 int b200_is_device_ptr(const void *p);
 void *b200_stream(void);
 int b200_set_thread_stream(void *stream);
+/* Makes `stream` the one b200_stream() returns on this thread (nullptr:
+ * back to the thread's own) and returns the previous override. */
+void *b200_override_stream(void *stream);
+/* A second stream paired with the calling thread's current stream, created
+ * on first use (nullptr when none can be had). */
+void *b200_aux_stream(void);
 int b200_stream_sync(void);
 int b200_alloc(void **p, size_t bytes);
 void b200_free(void *p);

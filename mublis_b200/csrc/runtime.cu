@@ -131,7 +131,40 @@ int b200_is_device_ptr(const void *p) {
   return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
+// A stream that library code switches to for part of one call (the
+// second column half of a large triangular solve); the thread's own stream
+// and its ownership are untouched.
+thread_local cudaStream_t t_override = nullptr;
+// Second streams, one per stream this thread issues on (a request server's
+// scheduler thread issues on several), so that concurrent calls on
+// different streams do not queue behind each other on a shared one.
+constexpr int AUX_SLOTS = 8;
+thread_local cudaStream_t t_aux_of[AUX_SLOTS] = {}, t_aux[AUX_SLOTS] = {};
+
+void *b200_override_stream(void *stream) {
+  void *prev = (void *)t_override;
+  t_override = (cudaStream_t)stream;
+  return prev;
+}
+
+void *b200_aux_stream(void) {
+  const cudaStream_t cur = (cudaStream_t)b200_stream();
+  int slot = -1;
+  for (int i = 0; i < AUX_SLOTS; ++i) {
+    if (t_aux[i] && t_aux_of[i] == cur) return (void *)t_aux[i];
+    if (!t_aux[i] && slot < 0) slot = i;
+  }
+  if (slot < 0) return nullptr;  // more primary streams than slots: no second stream
+  if (cudaStreamCreateWithFlags(&t_aux[slot], cudaStreamNonBlocking) != cudaSuccess) {
+    t_aux[slot] = nullptr;
+    return nullptr;
+  }
+  t_aux_of[slot] = cur;
+  return (void *)t_aux[slot];
+}
+
 void *b200_stream(void) {
+  if (t_override) return (void *)t_override;
   if (!t_stream) {
     cudaStreamCreateWithFlags(&t_stream, cudaStreamNonBlocking);
     t_stream_owned = true;

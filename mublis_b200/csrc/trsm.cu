@@ -183,11 +183,30 @@ int grow_inverse(const b200_trsm_desc_t *d, T *inv, T *tmp, const long big, cuda
   return B200_OK;
 }
 
+// One L3 product per column chain: chain c runs on streams[c] (the
+// thread's stream is overridden for it), so chains are enqueued in lockstep.
+struct Chains {
+  const b200_trsm_desc_t *d[2];
+  cudaStream_t streams[2];
+  int count;
+};
+
+template <typename Build>
+int for_each_chain(const Chains &ch, Build build) {
+  for (int c = 0; c < ch.count; ++c) {
+    b200_l3_desc_t g = build(*ch.d[c]);
+    void *prev = b200_override_stream((void *)ch.streams[c]);
+    const int st = b200_l3_run(&g);
+    b200_override_stream(prev);
+    B200_TRY(st);
+  }
+  return B200_OK;
+}
+
 template <typename T>
-int trsm_rec(const b200_trsm_desc_t *d, const T *inv, const long big, long r0, long r1) {
-  const T *a = (const T *)d->a;
-  T *b = (T *)d->b;
-  const bool lower = d->uplo == MUBLIS_LOWER;
+int trsm_rec(const Chains &ch, const T *inv, const long big, long r0, long r1) {
+  const b200_trsm_desc_t &d0 = *ch.d[0];
+  const bool lower = d0.uplo == MUBLIS_LOWER;
   long rows = r1 - r0;
   if (rows <= big) {
     // X_b = inv(A_bb) B_b in place: the packed path packs B_b before the
@@ -195,50 +214,57 @@ int trsm_rec(const b200_trsm_desc_t *d, const T *inv, const long big, long r0, l
     // (FP32) whatever form the updates use.  inv(A_bb) is triangular like
     // A_bb, so it goes in as a triangular operand with the matching k range
     // per row tile (pi LOWER / UPPER): the zero tiles are not multiplied.
-    b200_l3_desc_t g = plain_gemm_desc(d->dtype, B200_FORM_PLAIN, 0);
-    g.product.domain.pi = lower ? MUBLIS_L3_LOWER : MUBLIS_L3_UPPER;
-    g.product.a.struc = MUBLIS_STRUC_TRIANGULAR;
-    g.product.a.uplo = d->uplo;
-    g.m = (int)rows;
-    g.n = d->n;
-    g.k = (int)rows;
-    g.alpha = 1.0;
-    g.beta = 0.0;
-    g.a[0] = inv + (r0 / big) * big * big;
-    g.rs_a[0] = 1;
-    g.cs_a[0] = big;
-    g.b[0] = b + r0 * d->rs_b;
-    g.rs_b[0] = d->rs_b;
-    g.cs_b[0] = d->cs_b;
-    g.c = b + r0 * d->rs_b;
-    g.rs_c = d->rs_b;
-    g.cs_c = d->cs_b;
-    return b200_l3_run(&g);
+    return for_each_chain(ch, [&](const b200_trsm_desc_t &d) {
+      T *b = (T *)d.b;
+      b200_l3_desc_t g = plain_gemm_desc(d.dtype, B200_FORM_PLAIN, 0);
+      g.product.domain.pi = lower ? MUBLIS_L3_LOWER : MUBLIS_L3_UPPER;
+      g.product.a.struc = MUBLIS_STRUC_TRIANGULAR;
+      g.product.a.uplo = d.uplo;
+      g.m = (int)rows;
+      g.n = d.n;
+      g.k = (int)rows;
+      g.alpha = 1.0;
+      g.beta = 0.0;
+      g.a[0] = inv + (r0 / big) * big * big;
+      g.rs_a[0] = 1;
+      g.cs_a[0] = big;
+      g.b[0] = b + r0 * d.rs_b;
+      g.rs_b[0] = d.rs_b;
+      g.cs_b[0] = d.cs_b;
+      g.c = b + r0 * d.rs_b;
+      g.rs_c = d.rs_b;
+      g.cs_c = d.cs_b;
+      return g;
+    });
   }
   long half = b200_round_up((rows + 1) / 2, big);
   long mid = r0 + half;
   // Rows solved first (src) and rows updated by them (dst).
   long s0 = lower ? r0 : mid, s1 = lower ? mid : r1;
   long t0 = lower ? mid : r0, t1 = lower ? r1 : mid;
-  B200_TRY(trsm_rec<T>(d, inv, big, s0, s1));
-  b200_l3_desc_t g = plain_gemm_desc(d->dtype, d->form, d->slices);
-  g.policy_n = d->policy_n;
-  g.m = (int)(t1 - t0);
-  g.n = d->n;
-  g.k = (int)(s1 - s0);
-  g.alpha = -1.0;
-  g.beta = 1.0;
-  g.a[0] = a + t0 * d->rs_a + s0 * d->cs_a;
-  g.rs_a[0] = d->rs_a;
-  g.cs_a[0] = d->cs_a;
-  g.b[0] = b + s0 * d->rs_b;
-  g.rs_b[0] = d->rs_b;
-  g.cs_b[0] = d->cs_b;
-  g.c = b + t0 * d->rs_b;
-  g.rs_c = d->rs_b;
-  g.cs_c = d->cs_b;
-  B200_TRY(b200_l3_run(&g));
-  return trsm_rec<T>(d, inv, big, t0, t1);
+  B200_TRY(trsm_rec<T>(ch, inv, big, s0, s1));
+  B200_TRY(for_each_chain(ch, [&](const b200_trsm_desc_t &d) {
+    const T *a = (const T *)d.a;
+    T *b = (T *)d.b;
+    b200_l3_desc_t g = plain_gemm_desc(d.dtype, d.form, d.slices);
+    g.policy_n = d.policy_n;
+    g.m = (int)(t1 - t0);
+    g.n = d.n;
+    g.k = (int)(s1 - s0);
+    g.alpha = -1.0;
+    g.beta = 1.0;
+    g.a[0] = a + t0 * d.rs_a + s0 * d.cs_a;
+    g.rs_a[0] = d.rs_a;
+    g.cs_a[0] = d.cs_a;
+    g.b[0] = b + s0 * d.rs_b;
+    g.rs_b[0] = d.rs_b;
+    g.cs_b[0] = d.cs_b;
+    g.c = b + t0 * d.rs_b;
+    g.rs_c = d.rs_b;
+    g.cs_c = d.cs_b;
+    return g;
+  }));
+  return trsm_rec<T>(ch, inv, big, t0, t1);
 }
 
 template <typename T>
@@ -255,7 +281,40 @@ int trsm_solve(const b200_trsm_desc_t *d) {
     st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
                             d->unit_diag != 0, inv, (int)big, s);
   if (st == B200_OK) st = grow_inverse<T>(d, inv, tmp, big, s);
-  if (st == B200_OK) st = trsm_rec<T>(d, inv, big, 0, d->m);
+  if (st == B200_OK) {
+    // The right-hand sides are independent: a large solve runs its two
+    // column halves as two chains of the same launches on two streams, so
+    // one half's kernels fill the wave tails of the other's (every column
+    // is computed exactly as in one chain).
+    cudaStream_t s2 = d->n >= 2048 && d->m >= 2048 ? (cudaStream_t)b200_aux_stream() : nullptr;
+    if (s2) {
+      b200_trsm_desc_t h0 = *d, h1 = *d;
+      const long half = b200_round_up((d->n + 1) / 2, 128);
+      h0.policy_n = h1.policy_n = d->policy_n > 0 ? d->policy_n : d->n;
+      h0.n = (int)half;
+      h1.n = (int)(d->n - half);
+      h1.b = (T *)d->b + half * d->cs_b;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (cudaEventCreateWithFlags(&e0, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&e1, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventRecord(e0, s) != cudaSuccess || cudaStreamWaitEvent(s2, e0, 0) != cudaSuccess)
+        st = b200_set_error(B200_ECUDA, "trsm: stream fork failed");
+      if (st == B200_OK) {
+        const Chains ch = {{&h0, &h1}, {s, s2}, 2};
+        st = trsm_rec<T>(ch, inv, big, 0, d->m);
+      }
+      // Join even after a failure, so nothing of the second chain is left
+      // running on the scratch freed below.
+      if (e1 && (cudaEventRecord(e1, s2) != cudaSuccess ||
+                 cudaStreamWaitEvent(s, e1, 0) != cudaSuccess) && st == B200_OK)
+        st = b200_set_error(B200_ECUDA, "trsm: stream join failed");
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    } else {
+      const Chains ch = {{d, nullptr}, {s, nullptr}, 1};
+      st = trsm_rec<T>(ch, inv, big, 0, d->m);
+    }
+  }
   b200_free(tmp);
   b200_free(inv);
   return st;
