@@ -220,6 +220,12 @@ def workload_config(n: int) -> dict:
 
 # ---------------------------------------------------------------- device arm
 
+def tri_elements(n: int, block: int = 256) -> int:
+    """Elements of an n x n triangle as the host path stages it: blocks of
+    `block` columns, each from its first column's diagonal down."""
+    return sum((n - j0) * min(block, n - j0) for j0 in range(0, n, block))
+
+
 class Family:
     """The 18 calls of one step with their own operands."""
 
@@ -250,12 +256,24 @@ class Family:
                 if not device:
                     ops = [x.cpu().pin_memory() for x in ops]
                 self.calls.append((p, r, ops))
-                n2 = n * n * elt
+                # Bytes the host path moves: triangular / symmetric A and the
+                # SYRK / SYR2K C cross PCIe as their triangle only, in blocks
+                # of 256 columns (C both ways).
+                n2, t2 = n * n * elt, tri_elements(n) * elt
                 if r in ("trmm", "trsm"):
-                    self.h2d += 2 * n2
+                    self.h2d += t2 + n2
                     self.d2h += n2
+                elif r == "symm":
+                    self.h2d += t2 + 2 * n2
+                    self.d2h += n2
+                elif r == "syrk":
+                    self.h2d += n2 + t2
+                    self.d2h += t2
+                elif r == "syr2k":
+                    self.h2d += 2 * n2 + t2
+                    self.d2h += t2
                 else:
-                    self.h2d += (2 if r == "syrk" else 3) * n2
+                    self.h2d += 3 * n2
                     self.d2h += n2
         torch.cuda.synchronize()
 

@@ -86,7 +86,15 @@ typedef struct {
   int form;
   int slices;
   long policy_n; /* as in b200_l3_desc_t, passed to the update products */
+  const void *prep; /* diagonal inverses from b200_trsm_prepare, or NULL */
 } b200_trsm_desc_t;
+
+/* trsm.cu: the inverted diagonal blocks depend only on A, so a solve split
+ * into column panels builds them once (prepare, on the calling thread's
+ * stream), passes the result in each panel's desc (prep) and releases it
+ * after the last panel. */
+int b200_trsm_prepare(const b200_trsm_desc_t *d, void **prep);
+void b200_trsm_release(void *prep);
 
 /* runtime.cu */
 int b200_init(void);
@@ -141,6 +149,11 @@ int b200_colpipe_view_ok(long rows, long rs, long cs);
 int b200_colpipe_panels(long ncols, size_t bytes);
 int b200_column_pipeline(const b200_colpipe_t *p);
 
+#ifdef __CUDACC__
+/* Host-to-device 2-D copy on s; large ones split over two copy engines. */
+cudaError_t b200_h2d_2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                        size_t height, cudaStream_t s);
+#endif
 int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long rows, long cols,
                   size_t elt);
 int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,

@@ -25,8 +25,40 @@ void b200_stage_begin(b200_stage_set_t *ss, size_t elt) {
   ss->elt = elt;
 }
 
+/* Copies a staged view between host and device: the whole view, or the
+ * blocks of TRI_BLOCK columns of the device-side orientation restricted to
+ * the rows that hold the staged triangle. */
+enum { TRI_BLOCK = 256 };
+
+static int stage_copy(const b200_stage_t *s, size_t elt, int to_device) {
+  /* Device orientation: column-major R x C with leading dimension ld. */
+  const long R = s->transposed ? s->cols : s->rows, C = s->transposed ? s->rows : s->cols;
+  const long hrs = s->transposed ? s->cs : s->rs, hcs = s->transposed ? s->rs : s->cs;
+  int tri = s->tri;
+  if (s->transposed && tri) tri = tri == 1 ? 2 : 1;
+  const long bw = tri ? TRI_BLOCK : C;
+  for (long j0 = 0; j0 < C; j0 += bw) {
+    const long j1 = j0 + bw < C ? j0 + bw : C;
+    long i0 = 0, i1 = R;
+    if (tri == 1) i0 = j0 < R ? j0 : R; /* column <= row: rows from the block's first column */
+    if (tri == 2) i1 = j1 < R ? j1 : R; /* column >= row: rows up to the block's last column */
+    if (i1 <= i0) continue;
+    char *dev = (char *)s->dev + (size_t)(i0 + j0 * s->ld) * elt;
+    const char *host = (const char *)s->host + (i0 * hrs + j0 * hcs) * (long)elt;
+    int st = to_device ? b200_copy_h2d(dev, s->ld, host, hrs, hcs, i1 - i0, j1 - j0, elt)
+                       : b200_copy_d2h((void *)host, hrs, hcs, dev, s->ld, i1 - i0, j1 - j0, elt);
+    if (st != B200_OK) return st;
+  }
+  return B200_OK;
+}
+
 int b200_stage_view(b200_stage_set_t *ss, const void *p, long rows, long cols, long rs, long cs,
                     int copy_in, int out, b200_view_t *v) {
+  return b200_stage_view_tri(ss, p, rows, cols, rs, cs, copy_in, out, 0, v);
+}
+
+int b200_stage_view_tri(b200_stage_set_t *ss, const void *p, long rows, long cols, long rs,
+                        long cs, int copy_in, int out, int tri, b200_view_t *v) {
   v->ptr = (void *)p;
   v->rs = rs;
   v->cs = cs;
@@ -39,6 +71,15 @@ int b200_stage_view(b200_stage_set_t *ss, const void *p, long rows, long cols, l
     int same = views_same(s, p, rows, cols, rs, cs);
     int swapped = views_same(s, p, cols, rows, cs, rs);
     if (!same && !swapped) continue;
+    /* The same host matrix staged again: if this use needs more of it than
+     * the earlier one copied in, copy the whole view (and write back all of
+     * it: the whole device copy is then valid). */
+    const int want = !tri ? 0 : (same ? tri : (tri == 1 ? 2 : 1));
+    if (s->tri && s->tri != want) {
+      s->tri = 0;
+      int st = stage_copy(s, ss->elt, 1);
+      if (st != B200_OK) return st;
+    }
     s->out |= out;
     /* Device strides of the staged copy in the requested orientation. */
     long drs = s->transposed ? s->ld : 1, dcs = s->transposed ? 1 : s->ld;
@@ -58,15 +99,14 @@ int b200_stage_view(b200_stage_set_t *ss, const void *p, long rows, long cols, l
   s->rs = rs;
   s->cs = cs;
   s->out = out;
+  s->tri = rows == cols ? tri : 0;
   s->transposed = rs != 1 && cs == 1;
   s->ld = s->transposed ? cols : rows;
   int st = b200_alloc(&s->dev, (size_t)rows * (size_t)cols * ss->elt);
   if (st != B200_OK) return st;
   ss->n++;
   if (copy_in) {
-    st = s->transposed
-             ? b200_copy_h2d(s->dev, s->ld, p, cs, rs, cols, rows, ss->elt)
-             : b200_copy_h2d(s->dev, s->ld, p, rs, cs, rows, cols, ss->elt);
+    st = stage_copy(s, ss->elt, 1);
     if (st != B200_OK) return st;
   }
   v->ptr = s->dev;
@@ -79,11 +119,7 @@ int b200_stage_end(b200_stage_set_t *ss, int status) {
   for (int q = 0; q < ss->n && status == B200_OK; ++q) {
     b200_stage_t *s = &ss->st[q];
     if (!s->out) continue;
-    status = s->transposed
-                 ? b200_copy_d2h((void *)s->host, s->cs, s->rs, s->dev, s->ld, s->cols, s->rows,
-                                 ss->elt)
-                 : b200_copy_d2h((void *)s->host, s->rs, s->cs, s->dev, s->ld, s->rows, s->cols,
-                                 ss->elt);
+    status = stage_copy(s, ss->elt, 0);
   }
   int sync = b200_stream_sync();
   for (int q = 0; q < ss->n; ++q) b200_free(ss->st[q].dev);
@@ -93,6 +129,13 @@ int b200_stage_end(b200_stage_set_t *ss, int status) {
 }
 
 static size_t elt_of(int dtype) { return dtype == B200_F64 ? sizeof(double) : sizeof(float); }
+
+/* Staged triangle of a SYMMETRIC / TRIANGULAR operand (1 lower, 2 upper), 0
+ * for a general one. */
+static int operand_tri(const mublis_l3_operand_t *o) {
+  if (o->struc == MUBLIS_STRUC_GENERAL) return 0;
+  return o->uplo == MUBLIS_LOWER ? 1 : o->uplo == MUBLIS_UPPER ? 2 : 0;
+}
 
 /* ---- column-panel pipelining of host operands ----------------------------
  *
@@ -151,7 +194,8 @@ static int try_pipeline_l3(const b200_l3_desc_t *d, int *status) {
   b200_stage_begin(&ss, elt);
   b200_l3_desc_t dd = *d;
   b200_view_t v;
-  int st = b200_stage_view(&ss, d->a[0], d->m, d->k, d->rs_a[0], d->cs_a[0], 1, 0, &v);
+  int st = b200_stage_view_tri(&ss, d->a[0], d->m, d->k, d->rs_a[0], d->cs_a[0], 1, 0,
+                               operand_tri(&pr->a), &v);
   dd.a[0] = v.ptr;
   dd.rs_a[0] = v.rs;
   dd.cs_a[0] = v.cs;
@@ -183,22 +227,29 @@ int b200_front_l3(b200_l3_desc_t *d) {
   b200_l3_desc_t dd = *d;
   const int update = d->alpha != 0.0 && d->k > 0;
   b200_view_t v;
+  /* A symmetric or triangular operand is read in its stored triangle only,
+   * and a ji-restricted C is read (beta != 0) and written in its triangle
+   * only: just those triangles cross PCIe. */
+  const mublis_l3_product_t *pr = &d->product;
+  const int a_tri = operand_tri(&pr->a), b_tri = operand_tri(&pr->b);
+  const int c_tri = pr->domain.ji == MUBLIS_L3_LOWER ? 1 : pr->domain.ji == MUBLIS_L3_UPPER ? 2 : 0;
   for (int t = 0; t < d->npairs && update && st == B200_OK; ++t) {
-    st = b200_stage_view(&ss, d->a[t], d->m, d->k, d->rs_a[t], d->cs_a[t], 1, 0, &v);
+    st = b200_stage_view_tri(&ss, d->a[t], d->m, d->k, d->rs_a[t], d->cs_a[t], 1, 0, a_tri, &v);
     dd.a[t] = v.ptr;
     dd.rs_a[t] = v.rs;
     dd.cs_a[t] = v.cs;
     if (st != B200_OK) break;
-    st = b200_stage_view(&ss, d->b[t], d->k, d->n, d->rs_b[t], d->cs_b[t], 1, 0, &v);
+    st = b200_stage_view_tri(&ss, d->b[t], d->k, d->n, d->rs_b[t], d->cs_b[t], 1, 0, b_tri, &v);
     dd.b[t] = v.ptr;
     dd.rs_b[t] = v.rs;
     dd.cs_b[t] = v.cs;
   }
   if (st == B200_OK) {
-    /* C is read when beta != 0, and must be preserved outside the written
-     * triangle when ji restricts the output. */
-    int c_in = d->beta != 0.0 || d->product.domain.ji != MUBLIS_L3_ALL;
-    st = b200_stage_view(&ss, d->c, d->m, d->n, d->rs_c, d->cs_c, c_in, 1, &v);
+    /* A triangle-staged C is copied in even when beta == 0: the column
+     * blocks that straddle the diagonal also hold elements of the other
+     * triangle, which the write-back must return unchanged. */
+    st = b200_stage_view_tri(&ss, d->c, d->m, d->n, d->rs_c, d->cs_c,
+                             d->beta != 0.0 || c_tri != 0, 1, c_tri, &v);
     dd.c = v.ptr;
     dd.rs_c = v.rs;
     dd.cs_c = v.cs;
@@ -238,7 +289,9 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
     return b200_stage_end(&ss, st);
   }
   int ka = side == MUBLIS_LEFT ? m : n;
-  if (st == B200_OK) st = b200_stage_view(&ss, a, ka, ka, rs_a, cs_a, 1, 0, &va);
+  /* Only the stored triangle of A is read: only it crosses PCIe. */
+  if (st == B200_OK)
+    st = b200_stage_view_tri(&ss, a, ka, ka, rs_a, cs_a, 1, 0, uplo == MUBLIS_UPPER ? 2 : 1, &va);
   if (st != B200_OK) return b200_stage_end(&ss, st);
 
   long ars = va.rs, acs = va.cs;
@@ -326,7 +379,9 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
     return b200_stage_end(&ss, st);
   }
   int ka = side == MUBLIS_LEFT ? m : n;
-  if (st == B200_OK) st = b200_stage_view(&ss, a, ka, ka, rs_a, cs_a, 1, 0, &va);
+  /* Only the stored triangle of A is read: only it crosses PCIe. */
+  if (st == B200_OK)
+    st = b200_stage_view_tri(&ss, a, ka, ka, rs_a, cs_a, 1, 0, uplo == MUBLIS_UPPER ? 2 : 1, &va);
   if (st != B200_OK) return b200_stage_end(&ss, st);
 
   long brs = vb.rs, bcs = vb.cs, ars = va.rs, acs = va.cs;
@@ -363,7 +418,13 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
     p.out_read = 1;
     p.run = trsm_panel;
     p.ctx = &d;
-    st = b200_column_pipeline(&p);
+    /* The diagonal inverses depend on A only: built once for all panels. */
+    void *prep = NULL;
+    d.policy_n = n;
+    st = b200_trsm_prepare(&d, &prep);
+    d.prep = prep;
+    if (st == B200_OK) st = b200_column_pipeline(&p);
+    b200_trsm_release(prep);
     return b200_stage_end(&ss, st);
   }
   st = ss.n == 0 && b200_serve_attached() ? b200_serve_trsm(&d) : b200_trsm_run(&d);

@@ -25,6 +25,7 @@ typedef struct {
   void *dev;
   long ld;
   int out;
+  int tri; /* 0: the whole view; 1: only c <= r (lower); 2: only c >= r (upper) */
 } b200_stage_t;
 
 typedef struct {
@@ -39,6 +40,14 @@ void b200_stage_begin(b200_stage_set_t *ss, size_t elt);
  * b200_stage_end. */
 int b200_stage_view(b200_stage_set_t *ss, const void *p, long rows, long cols, long rs, long cs,
                     int copy_in, int out, b200_view_t *v);
+/* Same, for an operand of which the call reads (and, with out, writes) only
+ * one triangle (tri: 1 = elements with column <= row, 2 = column >= row):
+ * only that triangle crosses PCIe, in blocks of columns, both ways (the
+ * blocks that straddle the diagonal carry some of the other triangle, so an
+ * output staged this way must also be copied in).  The rest of the other
+ * triangle of the device copy is left unset and never copied back. */
+int b200_stage_view_tri(b200_stage_set_t *ss, const void *p, long rows, long cols, long rs,
+                        long cs, int copy_in, int out, int tri, b200_view_t *v);
 /* Copies outputs back (when status is OK), frees, synchronises. */
 int b200_stage_end(b200_stage_set_t *ss, int status);
 

@@ -124,6 +124,13 @@ int run_dmma(const b200_l3_desc_t *d) {
     std::vector<int2> flat(tl.size());
     for (size_t i = 0; i < tl.size(); ++i) flat[i] = tl[i].second;
     ntiles = (int)flat.size();
+    // The persistent CTAs take tiles round-robin (tile CTA + round * grid);
+    // with the list heaviest first, reversing every other round ("snake")
+    // evens out each CTA's total instead of giving CTA 0 the heaviest tile
+    // of every round.
+    const size_t grid = (size_t)std::min(ntiles, b200_sm_count());
+    for (size_t r0 = grid; grid > 0 && r0 < flat.size(); r0 += 2 * grid)
+      std::reverse(flat.begin() + r0, flat.begin() + std::min(flat.size(), r0 + grid));
     st = b200_alloc(&list, sizeof(int2) * (ntiles > 0 ? ntiles : 1));
     if (st == B200_OK && ntiles > 0 &&
         cudaMemcpyAsync(list, flat.data(), sizeof(int2) * ntiles, cudaMemcpyHostToDevice, s) !=

@@ -267,8 +267,14 @@ int trsm_rec(const Chains &ch, const T *inv, const long big, long r0, long r1) {
   return trsm_rec<T>(ch, inv, big, t0, t1);
 }
 
+// Inverted diagonal blocks of one triangle (the leaves of the solve).
+struct TrsmPrep {
+  void *inv;
+  long big;
+};
+
 template <typename T>
-int trsm_solve(const b200_trsm_desc_t *d) {
+int build_inverse(const b200_trsm_desc_t *d, TrsmPrep *p) {
   cudaStream_t s = b200_cur_stream();
   T *inv = nullptr, *tmp = nullptr;
   const long big = leaf_order(d->m, d->policy_n > 0 ? d->policy_n : d->n);
@@ -281,6 +287,28 @@ int trsm_solve(const b200_trsm_desc_t *d) {
     st = launch_inv_diag<T>(d->m, (const T *)d->a, d->rs_a, d->cs_a, d->uplo == MUBLIS_LOWER,
                             d->unit_diag != 0, inv, (int)big, s);
   if (st == B200_OK) st = grow_inverse<T>(d, inv, tmp, big, s);
+  b200_free(tmp);
+  if (st != B200_OK) {
+    b200_free(inv);
+    return st;
+  }
+  p->inv = inv;
+  p->big = big;
+  return B200_OK;
+}
+
+template <typename T>
+int trsm_solve(const b200_trsm_desc_t *d) {
+  cudaStream_t s = b200_cur_stream();
+  TrsmPrep own = {nullptr, 0};
+  const TrsmPrep *prep = (const TrsmPrep *)d->prep;
+  if (!prep) {
+    B200_TRY(build_inverse<T>(d, &own));
+    prep = &own;
+  }
+  const T *inv = (const T *)prep->inv;
+  const long big = prep->big;
+  int st = B200_OK;
   if (st == B200_OK) {
     // The right-hand sides are independent: a large solve runs its two
     // column halves as two chains of the same launches on two streams, so
@@ -315,12 +343,33 @@ int trsm_solve(const b200_trsm_desc_t *d) {
       st = trsm_rec<T>(ch, inv, big, 0, d->m);
     }
   }
-  b200_free(tmp);
-  b200_free(inv);
+  b200_free(own.inv);
   return st;
 }
 
 }  // namespace
+
+extern "C" int b200_trsm_prepare(const b200_trsm_desc_t *d, void **prep) {
+  *prep = nullptr;
+  if (d->m <= 0) return B200_OK;
+  if (d->uplo != MUBLIS_LOWER && d->uplo != MUBLIS_UPPER)
+    return b200_set_error(B200_EINVAL, "trsm: uplo must be lower or upper");
+  TrsmPrep *p = new TrsmPrep{nullptr, 0};
+  const int st = d->dtype == B200_F32 ? build_inverse<float>(d, p) : build_inverse<double>(d, p);
+  if (st != B200_OK) {
+    delete p;
+    return st;
+  }
+  *prep = p;
+  return B200_OK;
+}
+
+extern "C" void b200_trsm_release(void *prep) {
+  TrsmPrep *p = (TrsmPrep *)prep;
+  if (!p) return;
+  b200_free(p->inv);  // stream-ordered after the panels on this stream
+  delete p;
+}
 
 extern "C" int b200_trsm_run(const b200_trsm_desc_t *d) {
   if (d->m <= 0 || d->n <= 0) return B200_OK;
