@@ -69,6 +69,7 @@ typedef struct {
   long policy_n; /* n the "auto" policy decides on (0: n).  A column panel of a
                   * larger call carries the call's n, so every panel takes the
                   * form the whole call would. */
+  long policy_m; /* same for m (0: m): triangle panels cover fewer rows */
 } b200_l3_desc_t;
 
 /* Left-side solve op(A) X = alpha B, already normalised by the host layer
@@ -142,11 +143,16 @@ typedef struct {
   int (*run)(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
              void *out_dev, long out_rs, long out_cs);
   void *ctx;
+  long panel_min; /* narrowest panel worth computing (0: 1024 columns) */
+  int out_lower;  /* the output is a lower triangle: panel j0 moves only rows
+                     j0.. (out_dev is then element (j0, j0)); needs out_read */
 } b200_colpipe_t;
 int b200_colpipe_view_ok(long rows, long rs, long cs);
 /* Number of panels worth using for ncols columns of total bytes (< 2: do
  * not pipeline). */
 int b200_colpipe_panels(long ncols, size_t bytes);
+/* Same with panels of at least min_cols columns. */
+int b200_colpipe_panels_min(long ncols, size_t bytes, long min_cols);
 int b200_column_pipeline(const b200_colpipe_t *p);
 
 #ifdef __CUDACC__

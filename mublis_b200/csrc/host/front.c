@@ -130,6 +130,12 @@ int b200_stage_end(b200_stage_set_t *ss, int status) {
 
 static size_t elt_of(int dtype) { return dtype == B200_F64 ? sizeof(double) : sizeof(float); }
 
+/* A TRMM / TRSM panel is a whole triangular product or solve over the
+ * panel's columns: below 2048 columns its inner products get too narrow to
+ * fill the GPU (at n = 4096: 9.2 ms end to end for DTRSM with 1024-column
+ * panels). */
+enum { TRI_PANEL = 2048 };
+
 /* Staged triangle of a SYMMETRIC / TRIANGULAR operand (1 lower, 2 upper), 0
  * for a general one. */
 static int operand_tri(const mublis_l3_operand_t *o) {
@@ -165,6 +171,29 @@ static int l3_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, lon
   return b200_l3_run(&d);
 }
 
+/* Panel [j0, j0 + cols) of a lower-triangle output (SYRK / SYR2K): rows j0..
+ * of C against rows j0.. of every A_t and columns j0.. of every B_t.  The
+ * panel's C starts on the diagonal, so the ji relation is unchanged, and
+ * each element is computed exactly as in the whole call. */
+static int lower_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
+                       void *out_dev, long out_rs, long out_cs) {
+  (void)in_dev, (void)in_rs, (void)in_cs;
+  b200_l3_desc_t d = *(const b200_l3_desc_t *)ctx;
+  const size_t elt = d.dtype == B200_F64 ? sizeof(double) : sizeof(float);
+  if (d.policy_m <= 0) d.policy_m = d.m;
+  if (d.policy_n <= 0) d.policy_n = d.n;
+  for (int t = 0; t < d.npairs; ++t) {
+    d.a[t] = (const char *)d.a[t] + j0 * d.rs_a[t] * (long)elt;
+    d.b[t] = (const char *)d.b[t] + j0 * d.cs_b[t] * (long)elt;
+  }
+  d.m -= (int)j0;
+  d.n = (int)cols;
+  d.c = out_dev;
+  d.rs_c = out_rs;
+  d.cs_c = out_cs;
+  return b200_l3_run(&d);
+}
+
 static int trsm_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, long in_cs,
                       void *out_dev, long out_rs, long out_cs) {
   (void)j0, (void)in_dev, (void)in_rs, (void)in_cs;
@@ -175,6 +204,53 @@ static int trsm_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, l
   d.rs_b = out_rs;
   d.cs_b = out_cs;
   return b200_trsm_run(&d);
+}
+
+/* A one-pair product that writes only the lower triangle of a square C
+ * (SYRK) as a pipeline over triangle panels of C: the operands are staged
+ * whole, then each column panel of C below the diagonal is copied in,
+ * computed and copied back while its neighbours move (DSYRK 4096^2 end to
+ * end: 7.7 -> 7.1 ms).  Two-pair products (SYR2K, k doubled) are left
+ * whole: their later, shorter panels have too few of their long tiles to
+ * fill the GPU (DSYR2K: 12.4 -> 13.1 ms when pipelined).  0 when the call
+ * does not qualify. */
+static int try_pipeline_lower(const b200_l3_desc_t *d, int *status) {
+  const mublis_l3_product_t *pr = &d->product;
+  if (b200_serve_attached() || d->npairs != 1 || d->alpha == 0.0 || d->k <= 0 || d->m != d->n ||
+      pr->domain.ji != MUBLIS_L3_LOWER || pr->domain.jp != MUBLIS_L3_ALL ||
+      pr->domain.pi != MUBLIS_L3_ALL || pr->a.struc != MUBLIS_STRUC_GENERAL ||
+      pr->b.struc != MUBLIS_STRUC_GENERAL || !pipelinable(d->c, d->m, d->rs_c, d->cs_c))
+    return 0;
+  for (int t = 0; t < d->npairs; ++t)
+    if (d->a[t] == d->c || d->b[t] == d->c) return 0;
+  const size_t elt = elt_of(d->dtype);
+  if (b200_colpipe_panels(d->n, (size_t)d->m * d->n * elt / 2) < 2) return 0;
+  b200_stage_set_t ss;
+  b200_stage_begin(&ss, elt);
+  b200_l3_desc_t dd = *d;
+  b200_view_t v;
+  int st = B200_OK;
+  for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
+    st = b200_stage_view(&ss, d->a[t], d->m, d->k, d->rs_a[t], d->cs_a[t], 1, 0, &v);
+    dd.a[t] = v.ptr, dd.rs_a[t] = v.rs, dd.cs_a[t] = v.cs;
+    if (st == B200_OK)
+      st = b200_stage_view(&ss, d->b[t], d->k, d->n, d->rs_b[t], d->cs_b[t], 1, 0, &v);
+    dd.b[t] = v.ptr, dd.rs_b[t] = v.rs, dd.cs_b[t] = v.cs;
+  }
+  if (st == B200_OK) {
+    b200_colpipe_t p;
+    memset(&p, 0, sizeof p);
+    p.elt = elt;
+    p.ncols = d->n;
+    p.out.host = d->c, p.out.rows = d->m, p.out.rs = d->rs_c, p.out.cs = d->cs_c;
+    p.out_read = 1; /* the diagonal blocks hold upper elements to return unchanged */
+    p.out_lower = 1;
+    p.run = lower_panel;
+    p.ctx = &dd;
+    st = b200_column_pipeline(&p);
+  }
+  *status = b200_stage_end(&ss, st);
+  return 1;
 }
 
 /* The l3 call as a pipeline over the columns of C, or 0 when it does not
@@ -221,6 +297,7 @@ int b200_front_l3(b200_l3_desc_t *d) {
   int st = b200_init();
   if (st != B200_OK) return st;
   if (try_pipeline_l3(d, &st)) return st;
+  if (try_pipeline_lower(d, &st)) return st;
 
   b200_stage_set_t ss;
   b200_stage_begin(&ss, elt_of(d->dtype));
@@ -278,7 +355,7 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
    * through the device in column panels (B stays unstaged here). */
   const int piped = side == MUBLIS_LEFT && alpha != 0.0 && !b200_serve_attached() &&
                     pipelinable(b, m, rs_b, cs_b) &&
-                    b200_colpipe_panels(n, (size_t)m * n * elt_of(dtype)) >= 2;
+                    b200_colpipe_panels_min(n, (size_t)m * n * elt_of(dtype), TRI_PANEL) >= 2;
   if (piped) {
     vb.ptr = b, vb.rs = rs_b, vb.cs = cs_b;
   } else {
@@ -345,6 +422,7 @@ int b200_front_trmm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
     p.out_read = 1;
     p.run = l3_panel;
     p.ctx = &d;
+    p.panel_min = TRI_PANEL;
     st = b200_column_pipeline(&p);
     return b200_stage_end(&ss, st);
   }
@@ -368,7 +446,7 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
   const long rs_left = side == MUBLIS_LEFT ? rs_b : cs_b, cs_left = side == MUBLIS_LEFT ? cs_b : rs_b;
   const int piped = alpha != 0.0 && !b200_serve_attached() &&
                     pipelinable(b, m_left, rs_left, cs_left) &&
-                    b200_colpipe_panels(n_left, (size_t)m * n * elt_of(dtype)) >= 2;
+                    b200_colpipe_panels_min(n_left, (size_t)m * n * elt_of(dtype), TRI_PANEL) >= 2;
   if (piped) {
     vb.ptr = b, vb.rs = rs_b, vb.cs = cs_b;
   } else {
@@ -418,6 +496,7 @@ int b200_front_trsm(int dtype, mublis_side_t side, mublis_uplo_t uplo, mublis_tr
     p.out_read = 1;
     p.run = trsm_panel;
     p.ctx = &d;
+    p.panel_min = TRI_PANEL;
     /* The diagonal inverses depend on A only: built once for all panels. */
     void *prep = NULL;
     d.policy_n = n;

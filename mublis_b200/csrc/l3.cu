@@ -32,7 +32,8 @@ namespace {
 int resolve_form(const b200_l3_desc_t *d) {
   int f = d->form == B200_FORM_AUTO ? b200_get_default_form(d->dtype) : d->form;
   if (f == B200_FORM_POLICY) {
-    const long m = d->m, n = d->policy_n > 0 ? d->policy_n : d->n;
+    const long m = d->policy_m > 0 ? d->policy_m : d->m;
+    const long n = d->policy_n > 0 ? d->policy_n : d->n;
     const long k = (long)d->k * d->npairs;
     const long mn = m < n ? m : n;
     // FP32: fp16x3 (normwise error ~0.6x plain) where it is at least as fast

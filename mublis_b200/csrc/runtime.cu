@@ -378,14 +378,16 @@ struct PanelCopy {
   long off, drs, dcs;
 };
 
-PanelCopy panel_copy(const b200_colpipe_view_t &v, long j0, long cols, size_t elt) {
+// Rows [r0, v.rows) of panel [j0, j0 + cols) of a host view.
+PanelCopy panel_copy(const b200_colpipe_view_t &v, long j0, long cols, size_t elt, long r0 = 0) {
   PanelCopy c;
+  const long rows = v.rows - r0;
   if (v.rs == 1) {
-    c.width = v.rows * elt, c.height = cols, c.hpitch = (cols == 1 ? v.rows : v.cs) * elt;
-    c.dpitch = v.rows * elt, c.off = j0 * v.cs, c.drs = 1, c.dcs = v.rows;
+    c.width = rows * elt, c.height = cols, c.hpitch = (cols == 1 ? v.rows : v.cs) * elt;
+    c.dpitch = rows * elt, c.off = j0 * v.cs + r0, c.drs = 1, c.dcs = rows;
   } else {
-    c.width = cols * elt, c.height = v.rows, c.hpitch = v.rs * elt;
-    c.dpitch = cols * elt, c.off = j0, c.drs = cols, c.dcs = 1;
+    c.width = cols * elt, c.height = rows, c.hpitch = v.rs * elt;
+    c.dpitch = cols * elt, c.off = r0 * v.rs + j0, c.drs = cols, c.dcs = 1;
   }
   return c;
 }
@@ -396,16 +398,21 @@ int b200_colpipe_view_ok(long rows, long rs, long cs) {
   return rs == 1 ? cs >= rows : (cs == 1 && rs >= 1);
 }
 
-int b200_colpipe_panels(long ncols, size_t bytes) {
-  if (bytes < (32u << 20)) return 1;
-  long p = ncols / 1024;
+int b200_colpipe_panels_min(long ncols, size_t bytes, long min_cols) {
+  if (bytes < (32u << 20) || min_cols <= 0) return 1;
+  long p = ncols / min_cols;
   return (int)(p > 4 ? 4 : p);
+}
+
+int b200_colpipe_panels(long ncols, size_t bytes) {
+  return b200_colpipe_panels_min(ncols, bytes, 1024);
 }
 
 int b200_column_pipeline(const b200_colpipe_t *p) {
   B200_TRY(copy_streams());
   cudaStream_t sc = b200_cur_stream(), si = t_copy_in, so = t_copy_out;
-  const int npan = b200_colpipe_panels(p->ncols, 1ull << 40);
+  const int npan =
+      b200_colpipe_panels_min(p->ncols, 1ull << 40, p->panel_min > 0 ? p->panel_min : 1024);
   const long w = b200_round_up(b200_ceil_div(p->ncols, npan < 1 ? 1 : npan), 128);
   const bool has_in = p->in.host != nullptr;
   const size_t in_bytes = has_in ? (size_t)p->in.rows * w * p->elt : 0;
@@ -434,7 +441,7 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
       cudaStreamWaitEvent(si, ev[q][2], 0);
     }
     const PanelCopy ci = has_in ? panel_copy(p->in, j0, cols, p->elt) : PanelCopy{};
-    const PanelCopy co = panel_copy(p->out, j0, cols, p->elt);
+    const PanelCopy co = panel_copy(p->out, j0, cols, p->elt, p->out_lower ? j0 : 0);
     cudaError_t e = cudaSuccess;
     if (has_in)
       e = b200_h2d_2d(in_dev, ci.dpitch, (const char *)p->in.host + ci.off * p->elt, ci.hpitch,

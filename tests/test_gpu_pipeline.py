@@ -3,8 +3,8 @@ panels (host copy-in, arithmetic and copy-out of neighbouring panels
 overlapped on three streams).
 
 Every case is run twice through cblas_*: once on host numpy arrays (the
-pipelined path) and once on device copies of the same bytes (one call, no
-staging).  With the plain forms each output element is summed in the same
+pipelined or triangle-staged path) and once on device copies of the same
+bytes (one call, no staging).  With the plain forms each output element is summed in the same
 order whatever the panel width, so the two results must be bit-identical
 (the device path itself is checked against the oracle by the parity
 suite).
@@ -61,6 +61,18 @@ CASES = [
          ta=False, unit=False, alpha=0.75, seed=36),
     dict(routine="trsm", dtype="float64", order="F", m=4096, n=1024, right=True, lower=False,
          ta=True, unit=True, alpha=0.5, seed=37),
+    # lower-triangle outputs: C moves in triangle panels (copied in even for
+    # beta == 0, since the diagonal blocks carry upper elements)
+    dict(routine="syrk", dtype="float64", order="F", m=4096, n=4096, k=1024, ta=False,
+         lower=True, alpha=0.75, beta=0.25, seed=38),
+    dict(routine="syrk", dtype="float32", order="F", m=4096, n=4096, k=768, ta=True,
+         lower=True, alpha=1.0, beta=0.0, seed=39),
+    dict(routine="syr2k", dtype="float32", order="F", m=4096, n=4096, k=1536, ta=False,
+         lower=True, alpha=0.75, beta=0.25, seed=40),
+    # row-major lower is a column-major upper triangle: staged as a triangle,
+    # not pipelined
+    dict(routine="syr2k", dtype="float64", order="C", m=3072, n=3072, k=512, ta=True,
+         lower=True, alpha=0.5, beta=0.5, seed=41),
 ]
 
 
@@ -69,7 +81,7 @@ def test_pipelined_host_call_matches_device_call(lib, case):
     torch = pytest.importorskip("torch")
     if case["routine"] in ("gemm", "symm"):
         case.setdefault("k", case["m"])
-    else:
+    elif case["routine"] in ("trmm", "trsm"):
         case.setdefault("k", case["m"] if not case["right"] else case["n"])
     a, b, c0 = cs.build(case)
     host_out = c0.copy(order="K")
