@@ -417,10 +417,14 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
   const bool has_in = p->in.host != nullptr;
   const size_t in_bytes = has_in ? (size_t)p->in.rows * w * p->elt : 0;
   const size_t out_bytes = (size_t)p->out.rows * w * p->elt;
-  void *buf[2] = {nullptr, nullptr};
-  cudaEvent_t ev[2][3] = {};  // per slot: copied in, computed, copied out
+  // Three panel slots: panel J + 1 is copied in while J computes and J - 1
+  // is still being copied back (with two, J + 1's copy-in waited for J - 1's
+  // copy-back, leaving the host-to-device direction idle).
+  constexpr int SLOTS = 3;
+  void *buf[SLOTS] = {};
+  cudaEvent_t ev[SLOTS][3] = {};  // per slot: copied in, computed, copied out
   int st = B200_OK;
-  for (int q = 0; q < 2 && st == B200_OK; ++q) {
+  for (int q = 0; q < SLOTS && st == B200_OK; ++q) {
     st = b200_alloc(&buf[q], in_bytes + out_bytes);
     for (int e = 0; e < 3 && st == B200_OK; ++e)
       if (cudaEventCreateWithFlags(&ev[q][e], cudaEventDisableTiming) != cudaSuccess)
@@ -434,9 +438,9 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
   long issued = 0;
   for (long j0 = 0; j0 < p->ncols && st == B200_OK; j0 += w, ++issued) {
     const long cols = p->ncols - j0 < w ? p->ncols - j0 : w;
-    const int q = (int)(issued & 1);
+    const int q = (int)(issued % SLOTS);
     char *in_dev = (char *)buf[q], *out_dev = (char *)buf[q] + in_bytes;
-    if (issued >= 2) {  // the slot's previous panel has been computed and copied out
+    if (issued >= SLOTS) {  // the slot's previous panel has been computed and copied out
       cudaStreamWaitEvent(si, ev[q][1], 0);
       cudaStreamWaitEvent(si, ev[q][2], 0);
     }
@@ -470,7 +474,7 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
   cudaStreamSynchronize(si);
   cudaStreamSynchronize(so);
   const int sync = b200_stream_sync();
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < SLOTS; ++q) {
     b200_free(buf[q]);
     for (int e = 0; e < 3; ++e)
       if (ev[q][e]) cudaEventDestroy(ev[q][e]);
