@@ -172,7 +172,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 
     // Epilogue: accumulator e of block (i, j) is row g + 8 (e >> 1), column
-    // 2 t + (e & 1) of the 16 x 8 block.
+    // 2 t + (e & 1) of the 16 x 8 block.  The two C values of each pair of
+    // adjacent columns are loaded before either is stored: a load / store
+    // chain per element pays one memory round trip each (the compiler cannot
+    // move a load of C above a store to C).  Larger batches spill at the 168
+    // registers a 9-warp CTA allows (measured slower); this one took DGEMM
+    // from 32.4 to 33.2 TF/s at 4096^3 and from 34.1 to 34.9 at 8192^3.
     const long m0 = (long)tm * BM + wm * 64, n0 = (long)tn * BN + wn * 32;
     const double alpha = p.alpha, beta = p.beta;
 #pragma unroll
@@ -182,16 +187,23 @@ __global__ void __launch_bounds__(THREADS, 1)
         const long gi = m0 + i * 16 + g + 8 * h;
         if (gi >= p.m) continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < 4; ++j) {
+          double cv[2];
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const long gj = n0 + j * 8 + 2 * t + e;
+            const bool in = gj < p.n && b200_rel(p.ji, gj, gi);
+            cv[e] = in && beta != 0.0 ? p.c[gi * p.rs_c + gj * p.cs_c] : 0.0;
+          }
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const long gj = n0 + j * 8 + 2 * t + e;
             if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
-            double *cij = p.c + gi * p.rs_c + gj * p.cs_c;
             double v = alpha * acc[i][j][2 * h + e];
-            if (beta != 0.0) v = fma(beta, *cij, v);
-            *cij = v;
+            if (beta != 0.0) v = fma(beta, cv[e], v);
+            p.c[gi * p.rs_c + gj * p.cs_c] = v;
           }
+        }
       }
   }
 }
