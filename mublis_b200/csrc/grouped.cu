@@ -133,19 +133,32 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
       __syncthreads();
     }
 
+    // Per row, the TN loads of C are issued before its stores (one memory
+    // round trip per row rather than per element; small problems spend a
+    // large share of their time here).  The FP64 8 x 8 variant, already at
+    // 255 registers, keeps one element at a time.
+    constexpr bool ROW_BATCH = !(sizeof(T) == 8 && TM * TN >= 64);
     const T alpha = (T)e.alpha, beta = (T)e.beta;
     T *Cm = (T *)e.c;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
       const long gi = m0 + ty + 16 * i;
       if (gi >= e.m) continue;
+      T cv[TN];
+      if constexpr (ROW_BATCH) {
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+          const long gj = n0 + tx + 16 * j;
+          cv[j] = gj < e.n && beta != T(0) ? Cm[gi * e.rs_c + gj * e.cs_c] : T(0);
+        }
+      }
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
         const long gj = n0 + tx + 16 * j;
         if (gj >= e.n) continue;
         T *cij = Cm + gi * e.rs_c + gj * e.cs_c;
         T v = alpha * acc[i][j];
-        if (beta != T(0)) v = fma(beta, *cij, v);
+        if (beta != T(0)) v = fma(beta, ROW_BATCH ? cv[j] : *cij, v);
         *cij = v;
       }
     }
