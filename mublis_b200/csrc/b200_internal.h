@@ -134,6 +134,20 @@ typedef struct {
   const void *host; /* NULL: no such operand */
   long rows, rs, cs;
 } b200_colpipe_view_t;
+/* An operand moved in index blocks beside the panels: with panel
+ * [j0, j0 + cols), rows (by_cols = 0) or columns (by_cols = 1) j0 .. j0 +
+ * cols - 1 of the host view, all `extent` elements of the other dimension,
+ * go to the same indices of its whole device copy.  Host and device agree
+ * on the unit stride (rs == drs == 1 or cs == dcs == 1). */
+typedef struct {
+  const void *host;
+  long rs, cs;
+  void *dev;
+  long drs, dcs;
+  long extent;
+  int by_cols;
+} b200_colpipe_stream_t;
+enum { B200_COLPIPE_MAX_PANELS = 8, B200_COLPIPE_MAX_STREAMS = 4 };
 typedef struct {
   size_t elt;
   long ncols;
@@ -146,6 +160,11 @@ typedef struct {
   long panel_min; /* narrowest panel worth computing (0: 1024 columns) */
   int out_lower;  /* the output is a lower triangle: panel j0 moves only rows
                      j0.. (out_dev is then element (j0, j0)); needs out_read */
+  int nwidths;    /* > 0: explicit panel widths, left to right (else even panels) */
+  long widths[B200_COLPIPE_MAX_PANELS];
+  int reverse;    /* compute the panels right to left */
+  int nstreams;
+  b200_colpipe_stream_t streams[B200_COLPIPE_MAX_STREAMS];
 } b200_colpipe_t;
 int b200_colpipe_view_ok(long rows, long rs, long cs);
 /* Number of panels worth using for ncols columns of total bytes (< 2: do

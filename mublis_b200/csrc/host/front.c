@@ -206,40 +206,124 @@ static int trsm_panel(void *ctx, long j0, long cols, void *in_dev, long in_rs, l
   return b200_trsm_run(&d);
 }
 
+/* Predicted time of the right-to-left lower-triangle pipeline with panel
+ * widths w[0..np) (left to right) over an n x n lower C with k-deep
+ * products: per panel, its blocks of the `nbuf` streamed operands and its
+ * part of C cross PCIe one after another, its tiles run in rounds of
+ * `slots` once those have arrived and the previous panel is done, and its
+ * C goes back.  Seconds at 50 GB/s each way and `rate` flop/s. */
+static double lower_plan_time(const long *w, int np, long n, long k, int npairs, int nbuf,
+                              size_t elt, double rate, int slots) {
+  const double bw = 50e9, tile = 128.0;
+  const double round_s = 2.0 * tile * tile * (double)k * npairs / (rate / slots);
+  double t_in = 0, t_comp = 0, t_out = 0;
+  long j0 = n;
+  for (int q = np - 1; q >= 0; --q) {
+    j0 -= w[q];
+    const double rows = (double)(n - j0), cols = (double)w[q];
+    const double cbytes = (rows * cols - cols * cols / 2) * elt;
+    t_in += (cbytes + cols * (double)k * elt * nbuf) / bw;
+    const long tr = (n - j0 + 127) / 128, tc = (w[q] + 127) / 128;
+    const long tiles = tc * tr - tc * (tc - 1) / 2; /* lower tiles of the panel */
+    const long rounds = (tiles + slots - 1) / slots;
+    t_comp = (t_in > t_comp ? t_in : t_comp) + rounds * round_s;
+    t_out = (t_comp > t_out ? t_comp : t_out) + cbytes / bw;
+  }
+  return t_out;
+}
+
+/* Panel widths (multiples of n / 32, rounded to 128 columns) for the
+ * right-to-left lower pipeline: the split into 2..4 panels with the least
+ * predicted time.  The leftmost panel is the last one computed and copied
+ * back, and the tallest, so the best splits keep it narrow (n = 4096 FP64
+ * SYR2K: 512 | 640 | 896 | 2048).  Returns the panel count. */
+static int lower_plan(long n, long k, int npairs, int nbuf, int dtype, long *w) {
+  const size_t elt = elt_of(dtype);
+  const double rate = dtype == B200_F64 ? 28e12 : 48e12;
+  const int sms = b200_sm_count() > 0 ? b200_sm_count() : 148;
+  const int slots = dtype == B200_F64 ? sms : 2 * sms;
+  long u = (n / 32 + 127) / 128 * 128;
+  if (u < 128) u = 128;
+  const int units = (int)((n + u - 1) / u);
+  double best = -1;
+  int best_np = 0;
+  long c[4];
+  for (int a = 1; a < units; ++a)
+    for (int b = a; b <= units; ++b)
+      for (int e = b; e <= units; ++e) {
+        /* cuts at a <= b <= e < units; equal cuts merge panels */
+        const int cut[4] = {a, b, e, units};
+        int np = 0;
+        long prev = 0;
+        for (int q = 0; q < 4; ++q) {
+          const long x = cut[q] * u < n ? cut[q] * u : n;
+          if (x > prev) c[np++] = x - prev, prev = x;
+        }
+        if (np < 2 || prev != n) continue;
+        const double t = lower_plan_time(c, np, n, k, npairs, nbuf, elt, rate, slots);
+        if (best < 0 || t < best) {
+          best = t, best_np = np;
+          for (int q = 0; q < np; ++q) w[q] = c[q];
+        }
+      }
+  return best_np;
+}
+
 /* A one-pair product that writes only the lower triangle of a square C
- * (SYRK) as a pipeline over triangle panels of C: the operands are staged
- * whole, then each column panel of C below the diagonal is copied in,
- * computed and copied back while its neighbours move (DSYRK 4096^2 end to
- * end: 7.7 -> 7.1 ms).  Two-pair products (SYR2K, k doubled) are left
- * whole: their later, shorter panels have too few of their long tiles to
- * fill the GPU (DSYR2K: 12.4 -> 13.1 ms when pipelined).  0 when the call
- * does not qualify. */
+ * (SYRK) as a pipeline over triangle panels of C: each column panel of C
+ * below the diagonal is copied in, computed and copied back while its
+ * neighbours move.  The panels run right to left, so the panel at column
+ * j0 reads only rows j0.. of op(A) and columns j0.. of op(B): those
+ * operands move in blocks beside the panels instead of before them
+ * (streams), and the planner above picks the widths.  Two-pair products
+ * (SYR2K) run this way only when every host operand can be streamed: with
+ * the operands staged first, the pipeline lost to the whole call (DSYR2K
+ * 4096^2: 12.4 -> 13.1 ms).  0 when the call does not qualify. */
 static int try_pipeline_lower(const b200_l3_desc_t *d, int *status) {
   const mublis_l3_product_t *pr = &d->product;
-  if (b200_serve_attached() || d->npairs != 1 || d->alpha == 0.0 || d->k <= 0 || d->m != d->n ||
-      pr->domain.ji != MUBLIS_L3_LOWER || pr->domain.jp != MUBLIS_L3_ALL ||
+  if (b200_serve_attached() || d->npairs < 1 || d->npairs > 2 || d->alpha == 0.0 || d->k <= 0 ||
+      d->m != d->n || pr->domain.ji != MUBLIS_L3_LOWER || pr->domain.jp != MUBLIS_L3_ALL ||
       pr->domain.pi != MUBLIS_L3_ALL || pr->a.struc != MUBLIS_STRUC_GENERAL ||
       pr->b.struc != MUBLIS_STRUC_GENERAL || !pipelinable(d->c, d->m, d->rs_c, d->cs_c))
     return 0;
-  for (int t = 0; t < d->npairs; ++t)
+  /* Streaming needs a unit stride in every host operand. */
+  int stream = 1;
+  for (int t = 0; t < d->npairs; ++t) {
     if (d->a[t] == d->c || d->b[t] == d->c) return 0;
+    if (!b200_is_device_ptr(d->a[t]) && d->rs_a[t] != 1 && d->cs_a[t] != 1) stream = 0;
+    if (!b200_is_device_ptr(d->b[t]) && d->rs_b[t] != 1 && d->cs_b[t] != 1) stream = 0;
+  }
+  if (!stream && d->npairs != 1) return 0;
   const size_t elt = elt_of(d->dtype);
   if (b200_colpipe_panels(d->n, (size_t)d->m * d->n * elt / 2) < 2) return 0;
   b200_stage_set_t ss;
   b200_stage_begin(&ss, elt);
   b200_l3_desc_t dd = *d;
+  b200_colpipe_t p;
+  memset(&p, 0, sizeof p);
   b200_view_t v;
   int st = B200_OK;
-  for (int t = 0; t < d->npairs && st == B200_OK; ++t) {
-    st = b200_stage_view(&ss, d->a[t], d->m, d->k, d->rs_a[t], d->cs_a[t], 1, 0, &v);
-    dd.a[t] = v.ptr, dd.rs_a[t] = v.rs, dd.cs_a[t] = v.cs;
-    if (st == B200_OK)
-      st = b200_stage_view(&ss, d->b[t], d->k, d->n, d->rs_b[t], d->cs_b[t], 1, 0, &v);
-    dd.b[t] = v.ptr, dd.rs_b[t] = v.rs, dd.cs_b[t] = v.cs;
-  }
+  for (int t = 0; t < d->npairs && st == B200_OK; ++t)
+    for (int side = 0; side < 2 && st == B200_OK; ++side) {
+      const void *h = side ? d->b[t] : d->a[t];
+      const long rs = side ? d->rs_b[t] : d->rs_a[t], cs = side ? d->cs_b[t] : d->cs_a[t];
+      st = side ? b200_stage_view(&ss, h, d->k, d->n, rs, cs, !stream, 0, &v)
+                : b200_stage_view(&ss, h, d->m, d->k, rs, cs, !stream, 0, &v);
+      if (side)
+        dd.b[t] = v.ptr, dd.rs_b[t] = v.rs, dd.cs_b[t] = v.cs;
+      else
+        dd.a[t] = v.ptr, dd.rs_a[t] = v.rs, dd.cs_a[t] = v.cs;
+      if (st != B200_OK || !stream || v.ptr == h) continue; /* device-resident: not moved */
+      int seen = 0;
+      for (int q = 0; q < p.nstreams; ++q) seen |= p.streams[q].dev == v.ptr;
+      if (seen) continue; /* another view of a matrix already moving */
+      b200_colpipe_stream_t *s = &p.streams[p.nstreams++];
+      s->host = h, s->rs = rs, s->cs = cs;
+      s->dev = v.ptr, s->drs = v.rs, s->dcs = v.cs;
+      s->extent = d->k;
+      s->by_cols = side; /* rows j0.. of op(A), columns j0.. of op(B) */
+    }
   if (st == B200_OK) {
-    b200_colpipe_t p;
-    memset(&p, 0, sizeof p);
     p.elt = elt;
     p.ncols = d->n;
     p.out.host = d->c, p.out.rows = d->m, p.out.rs = d->rs_c, p.out.cs = d->cs_c;
@@ -247,6 +331,10 @@ static int try_pipeline_lower(const b200_l3_desc_t *d, int *status) {
     p.out_lower = 1;
     p.run = lower_panel;
     p.ctx = &dd;
+    if (stream) {
+      p.reverse = 1;
+      p.nwidths = lower_plan(d->n, d->k, d->npairs, p.nstreams, d->dtype, p.widths);
+    }
     st = b200_column_pipeline(&p);
   }
   *status = b200_stage_end(&ss, st);

@@ -411,9 +411,35 @@ int b200_colpipe_panels(long ncols, size_t bytes) {
 int b200_column_pipeline(const b200_colpipe_t *p) {
   B200_TRY(copy_streams());
   cudaStream_t sc = b200_cur_stream(), si = t_copy_in, so = t_copy_out;
-  const int npan =
-      b200_colpipe_panels_min(p->ncols, 1ull << 40, p->panel_min > 0 ? p->panel_min : 1024);
-  const long w = b200_round_up(b200_ceil_div(p->ncols, npan < 1 ? 1 : npan), 128);
+  // Panels [start[q], start[q] + width[q]), left to right.
+  long width[B200_COLPIPE_MAX_PANELS], start[B200_COLPIPE_MAX_PANELS];
+  int np = 0;
+  if (p->nwidths > 0) {
+    if (p->nwidths > B200_COLPIPE_MAX_PANELS)
+      return b200_set_error(B200_EINVAL, "pipeline: too many panels");
+    long sum = 0;
+    for (int q = 0; q < p->nwidths; ++q) {
+      if (p->widths[q] <= 0) return b200_set_error(B200_EINVAL, "pipeline: empty panel");
+      start[q] = sum, width[q] = p->widths[q], sum += p->widths[q];
+    }
+    if (sum != p->ncols) return b200_set_error(B200_EINVAL, "pipeline: panels do not cover C");
+    np = p->nwidths;
+  } else {
+    const int npan =
+        b200_colpipe_panels_min(p->ncols, 1ull << 40, p->panel_min > 0 ? p->panel_min : 1024);
+    const long w0 = b200_round_up(b200_ceil_div(p->ncols, npan < 1 ? 1 : npan), 128);
+    for (long j0 = 0; j0 < p->ncols && np < B200_COLPIPE_MAX_PANELS; j0 += w0, ++np)
+      start[np] = j0, width[np] = p->ncols - j0 < w0 ? p->ncols - j0 : w0;
+  }
+  if (p->nstreams < 0 || p->nstreams > B200_COLPIPE_MAX_STREAMS)
+    return b200_set_error(B200_EINVAL, "pipeline: too many streamed operands");
+  for (int t = 0; t < p->nstreams; ++t) {
+    const b200_colpipe_stream_t &s = p->streams[t];
+    if (!((s.rs == 1 && s.drs == 1) || (s.cs == 1 && s.dcs == 1)))
+      return b200_set_error(B200_EINVAL, "pipeline: streamed operand has no unit stride");
+  }
+  long w = 0;
+  for (int q = 0; q < np; ++q) w = width[q] > w ? width[q] : w;
   const bool has_in = p->in.host != nullptr;
   const size_t in_bytes = has_in ? (size_t)p->in.rows * w * p->elt : 0;
   const size_t out_bytes = (size_t)p->out.rows * w * p->elt;
@@ -436,8 +462,9 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
                         cudaStreamWaitEvent(si, ready, 0) != cudaSuccess))
     st = b200_set_error(B200_ECUDA, "pipeline: stream ordering failed");
   long issued = 0;
-  for (long j0 = 0; j0 < p->ncols && st == B200_OK; j0 += w, ++issued) {
-    const long cols = p->ncols - j0 < w ? p->ncols - j0 : w;
+  for (int pn = 0; pn < np && st == B200_OK; ++pn, ++issued) {
+    const int pq = p->reverse ? np - 1 - pn : pn;
+    const long j0 = start[pq], cols = width[pq];
     const int q = (int)(issued % SLOTS);
     char *in_dev = (char *)buf[q], *out_dev = (char *)buf[q] + in_bytes;
     if (issued >= SLOTS) {  // the slot's previous panel has been computed and copied out
@@ -447,7 +474,21 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
     const PanelCopy ci = has_in ? panel_copy(p->in, j0, cols, p->elt) : PanelCopy{};
     const PanelCopy co = panel_copy(p->out, j0, cols, p->elt, p->out_lower ? j0 : 0);
     cudaError_t e = cudaSuccess;
-    if (has_in)
+    // The streamed operands' blocks of this panel go first: the panel's
+    // arithmetic reads them (and, with reverse, the blocks of the panels
+    // to its right, which came earlier on the same stream).
+    for (int t = 0; t < p->nstreams && e == cudaSuccess; ++t) {
+      const b200_colpipe_stream_t &s = p->streams[t];
+      const long r0 = s.by_cols ? 0 : j0, c0 = s.by_cols ? j0 : 0;
+      const long nr = s.by_cols ? s.extent : cols, nc = s.by_cols ? cols : s.extent;
+      const char *src = (const char *)s.host + (r0 * s.rs + c0 * s.cs) * (long)p->elt;
+      char *dst = (char *)s.dev + (r0 * s.drs + c0 * s.dcs) * (long)p->elt;
+      if (s.rs == 1 && s.drs == 1)
+        e = b200_h2d_2d(dst, s.dcs * p->elt, src, s.cs * p->elt, nr * p->elt, nc, si);
+      else
+        e = b200_h2d_2d(dst, s.drs * p->elt, src, s.rs * p->elt, nc * p->elt, nr, si);
+    }
+    if (has_in && e == cudaSuccess)
       e = b200_h2d_2d(in_dev, ci.dpitch, (const char *)p->in.host + ci.off * p->elt, ci.hpitch,
                       ci.width, ci.height, si);
     if (e == cudaSuccess && p->out_read)
