@@ -399,16 +399,9 @@ def _log_uniform_int(rng, lo, hi, size):
     return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size))).astype(int)
 
 
-def grouped_study(torch, lib) -> dict:
-    """Config 4: 4096 independent SGEMMs with m, n, k log-uniform over [16, 512]
-    (seed 1), column-major, lda = m, per-problem alpha, beta uniform[0.5, 1.5);
-    and 1024 DTRSMs (left, lower, non-unit) with order log-uniform in [32, 256],
-    right-hand sides log-uniform in [1, 128], A off-diagonal uniform/n and
-    diagonal in [1, 2).  One persistent grouped launch per plan (tiles
-    autotuned, CUDA-graph replay) against one library call per problem."""
-    import numpy as np
+def _grouped_sgemms(torch, rng):
+    """Config 4's 4096 SGEMMs on the device: (problems, operand tensors, ctypes array)."""
     import mublis_b200 as mb
-    rng = np.random.default_rng(1)
     torch.manual_seed(1)
     mnk = _log_uniform_int(rng, 16, 512, (4096, 3))
     ab = rng.uniform(0.5, 1.5, (4096, 2))
@@ -421,8 +414,36 @@ def grouped_study(torch, lib) -> dict:
         probs.append(mb.GemmProblem(0, 0, m, n, k, ab[q, 0], ab[q, 1], a.data_ptr(), m,
                                     b.data_ptr(), k, c.data_ptr(), m))
         keep.append((a, b, c))
+    return probs, keep, (mb.GemmProblem * len(probs))(*probs)
+
+
+def grouped_direct(torch, lib) -> dict:
+    """Config 4's SGEMMs as direct grouped calls (no plan, no autotuning): one
+    warm-up call, then five timed, three kernel launches per call (one per
+    tile class).  For profiler captures of the grouped kernel."""
+    import numpy as np
+    import mublis_b200 as mb
+    probs, keep, arr = _grouped_sgemms(torch, np.random.default_rng(1))
     gflop = sum(2.0 * p.m * p.n * p.k for p in probs)
-    arr = (mb.GemmProblem * len(probs))(*probs)
+    mb.check(lib.mublis_b200_gemm_grouped(b"s", arr, len(probs)), lib)
+    ms = timed(torch, lambda: lib.mublis_b200_gemm_grouped(b"s", arr, len(probs)), 5)
+    del keep
+    return {"gflop": round(gflop / 1e9, 2), "ms": round(ms, 3),
+            "tflops": round(gflop / ms / 1e9, 2)}
+
+
+def grouped_study(torch, lib) -> dict:
+    """Config 4: 4096 independent SGEMMs with m, n, k log-uniform over [16, 512]
+    (seed 1), column-major, lda = m, per-problem alpha, beta uniform[0.5, 1.5);
+    and 1024 DTRSMs (left, lower, non-unit) with order log-uniform in [32, 256],
+    right-hand sides log-uniform in [1, 128], A off-diagonal uniform/n and
+    diagonal in [1, 2).  One persistent grouped launch per plan (tiles
+    autotuned, CUDA-graph replay) against one library call per problem."""
+    import numpy as np
+    import mublis_b200 as mb
+    rng = np.random.default_rng(1)
+    probs, keep, arr = _grouped_sgemms(torch, rng)
+    gflop = sum(2.0 * p.m * p.n * p.k for p in probs)
     plan = ctypes.c_void_p()
     mb.check(lib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)), lib)
     ms_plan = timed(torch, lambda: lib.mublis_b200_plan_run(plan), 10)
@@ -612,6 +633,8 @@ def main():
     ap.add_argument("--forms-n", type=int, default=8192)
     ap.add_argument("--only-sides", action="store_true",
                     help="run only the TRSM/TRMM side x uplo x transpose study")
+    ap.add_argument("--only-grouped", action="store_true",
+                    help="run only config 4's SGEMMs as direct grouped calls (profiler captures)")
     ap.add_argument("--only-timed", action="store_true",
                     help="warm-up + timed steps only (for profiler launch lists)")
     args = ap.parse_args()
@@ -644,6 +667,11 @@ def main():
     if args.only_sides:
         if rank == 0:
             print(json.dumps({"sides_tflops": sides_study(torch, lib, args.n), "n": args.n}))
+        return
+
+    if args.only_grouped:
+        if rank == 0:
+            print(json.dumps({"grouped_direct": grouped_direct(torch, lib)}))
         return
 
     if args.only_forms:

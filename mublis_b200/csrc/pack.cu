@@ -141,6 +141,58 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
   }
 }
 
+// General operands copied as stored (no structure, no domain mask, no
+// transform into planes): the plain forms' common case, without
+// pack_kernel's per-element structure checks.  A CTA moves 32 (mn) x 64
+// (kk) elements with eight loads in flight per thread; tiles wholly inside
+// the view skip the bounds checks.  Positive strides, mn_pad a multiple of
+// 32.  The panel is the one pack_kernel writes for the same view.
+template <typename T, bool MN_CONTIG>
+__global__ void __launch_bounds__(256)
+    pack_dense_kernel(const T *__restrict__ x, long mn_stride, long kk_stride, long mn_len,
+                      long k_len, long kk0, long kk1, PackOut o) {
+  __shared__ T tile[64][33];  // [kk_local][mn_local]
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const long mn_base = (long)blockIdx.x * 32;
+  const long kk_base = kk0 + (long)blockIdx.y * 64;
+  const long kend = kk1 < kk0 + k_len ? kk1 : kk0 + k_len;  // zeros from here on
+  const bool full = mn_base + 32 <= mn_len && kk_base + 64 <= kend;
+  const T *src = x + mn_base * mn_stride + (kk_base - kk0) * kk_stride;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    // Lanes run along the source's unit-stride dimension.
+    const int mn_l = MN_CONTIG ? tx : ty + 8 * (q & 3);
+    const int kk_l = MN_CONTIG ? ty + 8 * q : tx + 32 * (q >> 2);
+    T val = T(0);
+    if (full || (mn_base + mn_l < mn_len && kk_base + kk_l < kend))
+      val = src[mn_l * mn_stride + kk_l * kk_stride];
+    tile[kk_l][mn_l] = val;
+  }
+  __syncthreads();
+  if (o.layout == PACK_FRAG64) {
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int combo = ty + 8 * q;  // 2 blocks of 16 rows x 16 k-quads
+        const int mn_l = (combo & 1) * 16 + (tx >> 2), kk_l = (combo >> 1) * 4 + (tx & 3);
+        const long kk = kk_base + kk_l;
+        if (kk >= kk1) continue;
+        *reinterpret_cast<double2 *>((double *)o.out +
+                                     b200_frag64_offset(mn_base + mn_l, kk, o.ld)) =
+            make_double2(tile[kk_l][mn_l], tile[kk_l][mn_l + 8]);
+      }
+    }
+    return;
+  }
+  T *out = (T *)o.out + mn_base + tx;  // PACK_MN_MAJOR
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int kk_l = ty + 8 * q;
+    const long kk = kk_base + kk_l;
+    if (kk < kk1) out[kk * o.ld] = tile[kk_l][tx];
+  }
+}
+
 // K-major panels (the tensor-core forms): a CTA covers 32 rows (mn) x 64 k.
 // Each thread turns 8 consecutive k of one row into every output plane and
 // writes them as one vector per plane (16 bytes of bf16, 8 bytes of int8,
@@ -473,6 +525,23 @@ int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn
     dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 64));
     if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
     pack_kmajor_kernel<T><<<grid, 256, 0, s>>>(v, b_side, mn_len, k_len, kk0, kk1, o, mn_fast);
+    B200_LAUNCH_CHECK();
+    return B200_OK;
+  }
+  const bool plain_copy = v.struc == MUBLIS_STRUC_GENERAL && v.mask_rel == MUBLIS_L3_ALL &&
+                          o.xform == PACK_COPY && mn_stride > 0 && kk_stride > 0 &&
+                          mn_pad % 32 == 0 &&
+                          (o.layout == PACK_MN_MAJOR || (o.layout == PACK_FRAG64 && sizeof(T) == 8));
+  if (plain_copy) {
+    dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 64));
+    if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
+    const T *x = (const T *)v.x;
+    if (mn_fast)
+      pack_dense_kernel<T, true>
+          <<<grid, 256, 0, s>>>(x, mn_stride, kk_stride, mn_len, k_len, kk0, kk1, o);
+    else
+      pack_dense_kernel<T, false>
+          <<<grid, 256, 0, s>>>(x, mn_stride, kk_stride, mn_len, k_len, kk0, kk1, o);
     B200_LAUNCH_CHECK();
     return B200_OK;
   }
