@@ -42,6 +42,22 @@ struct GemmEntry {
 // covers (16*TM) x (16*TN).  Double-buffered shared memory with register
 // prefetch of the next k-block; loads follow whichever operand stride is 1.
 
+// Copies a run of V elements from shared memory (16- or 8-byte aligned when
+// the run is that long) into registers with one vector load.
+template <typename T, int V>
+__device__ __forceinline__ void lds_run(T *dst, const T *src) {
+  if constexpr (V * sizeof(T) == 16) {
+    const uint4 x = *reinterpret_cast<const uint4 *>(src);
+    memcpy(dst, &x, 16);
+  } else if constexpr (V * sizeof(T) == 8) {
+    const uint2 x = *reinterpret_cast<const uint2 *>(src);
+    memcpy(dst, &x, 8);
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) dst[v] = src[v];
+  }
+}
+
 // `table` may be null: then the single problem `one` (passed by value in the
 // launch parameters) is the whole group -- the direct path for one small GEMM,
 // with no table upload.
@@ -54,15 +70,18 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
   __shared__ __align__(16) T As[2][BK][BM];
   __shared__ __align__(16) T Bs[2][BK][BN];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // Thread (tx, ty) holds rows row0 + (i % VM) + 16 VM (i / VM) and columns
+  // col0 + (j % VN) + 16 VN (j / VN): runs of up to 16 bytes, so each k step
+  // reads its A and B fragments with vector shared loads (one 16-byte load
+  // per four floats instead of four 4-byte loads).
+  constexpr int VM = TM * sizeof(T) >= 16 ? 16 / (int)sizeof(T) : TM;
+  constexpr int VN = TN * sizeof(T) >= 16 ? 16 / (int)sizeof(T) : TN;
+  const int row0 = ty * VM, col0 = tx * VN;
 
+  // The table is followed by one int per output tile: the tile's problem.
+  const int *tile_prob = table ? reinterpret_cast<const int *>(table + nprob) : nullptr;
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    // problem of this tile: last entry with tile0 <= tile
-    int lo = 0, hi = nprob - 1;
-    while (table && lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (table[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
-    }
-    const GemmEntry &e = table ? table[lo] : one;
+    const GemmEntry &e = table ? table[tile_prob[tile]] : one;
     const int local = tile - e.tile0;
     const long m0 = (long)(local % e.tiles_m) * BM, n0 = (long)(local / e.tiles_m) * BN;
     const T *A = (const T *)e.a, *B = (const T *)e.b;
@@ -121,9 +140,9 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
       for (int p = 0; p < BK; ++p) {
         T af[TM], bf[TN];
 #pragma unroll
-        for (int i = 0; i < TM; ++i) af[i] = As[cur][p][ty + 16 * i];
+        for (int g = 0; g < TM / VM; ++g) lds_run<T, VM>(af + g * VM, &As[cur][p][row0 + 16 * VM * g]);
 #pragma unroll
-        for (int j = 0; j < TN; ++j) bf[j] = Bs[cur][p][tx + 16 * j];
+        for (int g = 0; g < TN / VN; ++g) lds_run<T, VN>(bf + g * VN, &Bs[cur][p][col0 + 16 * VN * g]);
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -142,19 +161,19 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
     T *Cm = (T *)e.c;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
-      const long gi = m0 + ty + 16 * i;
+      const long gi = m0 + row0 + i % VM + 16 * VM * (i / VM);
       if (gi >= e.m) continue;
       T cv[TN];
       if constexpr (ROW_BATCH) {
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
-          const long gj = n0 + tx + 16 * j;
+          const long gj = n0 + col0 + j % VN + 16 * VN * (j / VN);
           cv[j] = gj < e.n && beta != T(0) ? Cm[gi * e.rs_c + gj * e.cs_c] : T(0);
         }
       }
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
-        const long gj = n0 + tx + 16 * j;
+        const long gj = n0 + col0 + j % VN + 16 * VN * (j / VN);
         if (gj >= e.n) continue;
         T *cij = Cm + gi * e.rs_c + gj * e.cs_c;
         T v = alpha * acc[i][j];
@@ -297,26 +316,50 @@ constexpr int NCLASS = 3;
 
 struct GemmGroup {
   std::vector<GemmEntry> entries;  // host copy, tile0/tiles_m filled for `variant`
-  GemmEntry *dtable = nullptr;
+  GemmEntry *dtable = nullptr;     // entries, then the tile -> problem map
+  size_t bytes = 0;                // allocated at dtable
   int tiles = 0;
   int variant = TILE_64;
 };
+
+// Host image of a class's device table for tile variant v: the entries
+// (tile0 / tiles_m filled) followed by one int per output tile, the index
+// of the tile's problem, so that a CTA finds its tile's problem with one
+// load (a binary search over tile0 was a chain of ~12 dependent loads per
+// tile).
+std::vector<char> table_image(std::vector<GemmEntry> &es, int v, int &tiles) {
+  int t = 0;
+  for (auto &e : es) {
+    e.tile0 = t;
+    e.tiles_m = (int)b200_ceil_div(e.m, kTileBM[v]);
+    t += e.tiles_m * (int)b200_ceil_div(e.n, kTileBN[v]);
+  }
+  tiles = t;
+  const size_t head = sizeof(GemmEntry) * es.size();
+  std::vector<char> img(head + sizeof(int) * (size_t)t);
+  if (!es.empty()) memcpy(img.data(), es.data(), head);
+  int *map = reinterpret_cast<int *>(img.data() + head);
+  for (size_t q = 0; q < es.size(); ++q) {
+    const int end = q + 1 < es.size() ? es[q + 1].tile0 : t;
+    for (int x = es[q].tile0; x < end; ++x) map[x] = (int)q;
+  }
+  return img;
+}
 
 // Builds the device table of one class for a tile variant.
 int build_group(std::vector<GemmEntry> &src, int variant, GemmGroup &g, cudaStream_t s) {
   g.entries = src;
   g.variant = variant;
-  int t = 0;
-  for (auto &e : g.entries) {
-    e.tile0 = t;
-    e.tiles_m = (int)b200_ceil_div(e.m, kTileBM[variant]);
-    t += e.tiles_m * (int)b200_ceil_div(e.n, kTileBN[variant]);
-  }
-  g.tiles = t;
+  const std::vector<char> img = table_image(g.entries, variant, g.tiles);
   if (g.entries.empty()) return B200_OK;
-  if (!g.dtable) B200_TRY(b200_alloc((void **)&g.dtable, sizeof(GemmEntry) * g.entries.size()));
-  B200_CUDA_TRY(cudaMemcpyAsync(g.dtable, g.entries.data(), sizeof(GemmEntry) * g.entries.size(),
-                                cudaMemcpyHostToDevice, s));
+  if (img.size() > g.bytes) {  // stream-ordered: earlier launches keep the old table
+    b200_free(g.dtable);
+    g.dtable = nullptr;
+    g.bytes = 0;
+    B200_TRY(b200_alloc((void **)&g.dtable, img.size()));
+    g.bytes = img.size();
+  }
+  B200_CUDA_TRY(cudaMemcpyAsync(g.dtable, img.data(), img.size(), cudaMemcpyHostToDevice, s));
   return B200_OK;
 }
 
@@ -711,17 +754,10 @@ extern "C" int b200_grouped_gemm_async(int dtype, const b200_l3_desc_t *const *d
     if (!tuned) v = fill_variant(cls[c], v);
     g[c].entries = cls[c];
     g[c].variant = v;
-    int t = 0;
-    for (auto &e : g[c].entries) {
-      e.tile0 = t;
-      e.tiles_m = (int)b200_ceil_div(e.m, kTileBM[v]);
-      t += e.tiles_m * (int)b200_ceil_div(e.n, kTileBN[v]);
-    }
-    g[c].tiles = t;
-    if (cudaMallocAsync((void **)&g[c].dtable, sizeof(GemmEntry) * g[c].entries.size(), s) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(g[c].dtable, g[c].entries.data(), sizeof(GemmEntry) * g[c].entries.size(),
-                        cudaMemcpyHostToDevice, s) != cudaSuccess)
+    const std::vector<char> img = table_image(g[c].entries, v, g[c].tiles);
+    if (cudaMallocAsync((void **)&g[c].dtable, img.size(), s) != cudaSuccess ||
+        cudaMemcpyAsync(g[c].dtable, img.data(), img.size(), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess)
       st = b200_set_error(B200_ECUDA, "grouped: table upload failed");
   }
   if (st == B200_OK)
