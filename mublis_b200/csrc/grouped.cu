@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -120,11 +121,20 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
       }
     };
 
-    T acc[TM][TN];
+    // FP32 accumulates column pairs with the packed sm_100 FMA (__ffma2_rn:
+    // two correctly rounded fmaf per instruction), halving the FMA issue
+    // slots; each element's result is that of fmaf.
+    constexpr bool PAIR = sizeof(T) == 4;
+    constexpr int TNP = PAIR ? TN / 2 : TN;
+    using Acc = typename std::conditional<PAIR, float2, T>::type;
+    Acc acc[TM][TNP];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
-      for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+      for (int j = 0; j < TNP; ++j) {
+        if constexpr (PAIR) acc[i][j] = make_float2(0.f, 0.f);
+        else acc[i][j] = T(0);
+      }
 
     const int kblocks = (int)((e.k + BK - 1) / BK);
     __syncthreads();  // previous tile's readers are done with the buffers
@@ -146,7 +156,13 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
-          for (int j = 0; j < TN; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+          for (int j = 0; j < TNP; ++j) {
+            if constexpr (PAIR)
+              acc[i][j] = __ffma2_rn(make_float2(af[i], af[i]),
+                                     make_float2(bf[2 * j], bf[2 * j + 1]), acc[i][j]);
+            else
+              acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+          }
       }
       if (kb + 1 < kblocks) sstore(cur ^ 1);
       __syncthreads();
@@ -176,7 +192,10 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
         const long gj = n0 + col0 + j % VN + 16 * VN * (j / VN);
         if (gj >= e.n) continue;
         T *cij = Cm + gi * e.rs_c + gj * e.cs_c;
-        T v = alpha * acc[i][j];
+        T aij;
+        if constexpr (PAIR) aij = (j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x;
+        else aij = acc[i][j];
+        T v = alpha * aij;
         if (beta != T(0)) v = fma(beta, ROW_BATCH ? cv[j] : *cij, v);
         *cij = v;
       }
@@ -212,13 +231,10 @@ __global__ void __launch_bounds__(256) grouped_trsm_kernel(const TrsmEntry *__re
   T(*X)[TRSM_SLAB + 1] = reinterpret_cast<T(*)[TRSM_SLAB + 1]>(trsm_smem);
   T(*L)[33] = reinterpret_cast<T(*)[33]>(trsm_smem + sizeof(T) * TRSM_MAX_ORDER * (TRSM_SLAB + 1));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // The table is followed by one int per slab: the slab's problem.
+  const int *slab_prob = reinterpret_cast<const int *>(table + nprob);
   for (int slab = blockIdx.x; slab < total_slabs; slab += gridDim.x) {
-    int lo = 0, hi = nprob - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (table[mid].slab0 <= slab) lo = mid; else hi = mid - 1;
-    }
-    const TrsmEntry &e = table[lo];
+    const TrsmEntry &e = table[slab_prob[slab]];
     const long j0 = (long)(slab - e.slab0) * TRSM_SLAB;
     const int ncol = (int)min((long)TRSM_SLAB, e.n - j0);
     const int m = (int)e.m;
@@ -551,10 +567,24 @@ int autotune(std::vector<GemmEntry> (&cls)[NCLASS], GemmGroup (&g)[NCLASS], cuda
 
 struct TrsmGroup {
   std::vector<TrsmEntry> entries;
-  TrsmEntry *dtable = nullptr;
+  TrsmEntry *dtable = nullptr;  // entries, then the slab -> problem map
   int slabs = 0;
   std::vector<int> fallback;  // problems too large for the one-CTA solve
 };
+
+// Host image of a TRSM group's device table: the entries followed by one
+// int per 32-column slab, the index of the slab's problem.
+std::vector<char> trsm_table_image(const TrsmGroup &g) {
+  const size_t head = sizeof(TrsmEntry) * g.entries.size();
+  std::vector<char> img(head + sizeof(int) * (size_t)g.slabs);
+  if (!g.entries.empty()) memcpy(img.data(), g.entries.data(), head);
+  int *map = reinterpret_cast<int *>(img.data() + head);
+  for (size_t q = 0; q < g.entries.size(); ++q) {
+    const int end = q + 1 < g.entries.size() ? g.entries[q + 1].slab0 : g.slabs;
+    for (int x = g.entries[q].slab0; x < end; ++x) map[x] = (int)q;
+  }
+  return img;
+}
 
 int to_trsm(const mublis_b200_trsm_problem_t *p, int count, TrsmGroup &g, cudaStream_t s) {
   int slabs = 0;
@@ -591,9 +621,9 @@ int to_trsm(const mublis_b200_trsm_problem_t *p, int count, TrsmGroup &g, cudaSt
   }
   g.slabs = slabs;
   if (g.entries.empty()) return B200_OK;
-  B200_TRY(b200_alloc((void **)&g.dtable, sizeof(TrsmEntry) * g.entries.size()));
-  B200_CUDA_TRY(cudaMemcpyAsync(g.dtable, g.entries.data(), sizeof(TrsmEntry) * g.entries.size(),
-                                cudaMemcpyHostToDevice, s));
+  const std::vector<char> img = trsm_table_image(g);
+  B200_TRY(b200_alloc((void **)&g.dtable, img.size()));
+  B200_CUDA_TRY(cudaMemcpyAsync(g.dtable, img.data(), img.size(), cudaMemcpyHostToDevice, s));
   return B200_OK;
 }
 
@@ -834,9 +864,9 @@ extern "C" int b200_grouped_trsm_async(int dtype, const b200_trsm_desc_t *const 
   }
   g.slabs = slabs;
   if (g.entries.empty()) return B200_OK;
-  if (cudaMallocAsync((void **)&g.dtable, sizeof(TrsmEntry) * g.entries.size(), s) != cudaSuccess ||
-      cudaMemcpyAsync(g.dtable, g.entries.data(), sizeof(TrsmEntry) * g.entries.size(),
-                      cudaMemcpyHostToDevice, s) != cudaSuccess)
+  const std::vector<char> img = trsm_table_image(g);
+  if (cudaMallocAsync((void **)&g.dtable, img.size(), s) != cudaSuccess ||
+      cudaMemcpyAsync(g.dtable, img.data(), img.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return b200_set_error(B200_ECUDA, "grouped: table upload failed");
   int st = dtype == B200_F64 ? launch_trsm_group<double>(g, s) : launch_trsm_group<float>(g, s);
   cudaFreeAsync(g.dtable, s);
