@@ -256,10 +256,13 @@ class Family:
                 if not device:
                     ops = [x.cpu().pin_memory() for x in ops]
                 self.calls.append((p, r, ops))
-                # Bytes the host path moves: triangular / symmetric A and the
-                # SYRK / SYR2K C cross PCIe as their triangle only, in blocks
-                # of 256 columns (C both ways).
+                # Bytes the host path moves: triangular / symmetric A cross
+                # PCIe as their triangle only, in blocks of 256 columns; the
+                # SYRK / SYR2K C (both ways) in the lower-triangle pipeline's
+                # blocks of 128 columns.
                 n2, t2 = n * n * elt, tri_elements(n) * elt
+                piped = n >= 2048 and n * n * elt // 2 >= 32 << 20
+                c2 = tri_elements(n, 128 if piped else 256) * elt
                 if r in ("trmm", "trsm"):
                     self.h2d += t2 + n2
                     self.d2h += n2
@@ -267,11 +270,11 @@ class Family:
                     self.h2d += t2 + 2 * n2
                     self.d2h += n2
                 elif r == "syrk":
-                    self.h2d += n2 + t2
-                    self.d2h += t2
+                    self.h2d += n2 + c2
+                    self.d2h += c2
                 elif r == "syr2k":
-                    self.h2d += 2 * n2 + t2
-                    self.d2h += t2
+                    self.h2d += 2 * n2 + c2
+                    self.d2h += c2
                 else:
                     self.h2d += 3 * n2
                     self.d2h += n2

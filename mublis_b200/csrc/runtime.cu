@@ -392,6 +392,31 @@ PanelCopy panel_copy(const b200_colpipe_view_t &v, long j0, long cols, size_t el
   return c;
 }
 
+// A lower-triangle output panel [j0, j0 + cols) (device panel from element
+// (j0, j0), strides co.drs / co.dcs) moved in blocks of 128 columns, each
+// from its first column's diagonal down, so the part of the panel's
+// diagonal block above the diagonal crosses PCIe only within 128 x 128
+// squares.
+cudaError_t lower_panel_copy(const b200_colpipe_view_t &v, long j0, long cols, size_t elt,
+                             void *dev, const PanelCopy &co, bool to_device, cudaStream_t s) {
+  constexpr long SUB = 128;
+  for (long c0 = j0; c0 < j0 + cols; c0 += SUB) {
+    const long nc = j0 + cols - c0 < SUB ? j0 + cols - c0 : SUB, nr = v.rows - c0;
+    if (nr <= 0) break;
+    char *d = (char *)dev + ((c0 - j0) * co.drs + (c0 - j0) * co.dcs) * (long)elt;
+    char *h = (char *)v.host + (c0 * v.rs + c0 * v.cs) * (long)elt;
+    const bool colmajor = v.rs == 1;
+    const size_t width = (colmajor ? nr : nc) * elt, height = colmajor ? nc : nr;
+    const size_t hpitch = (colmajor ? v.cs : v.rs) * elt;
+    const size_t dpitch = (colmajor ? co.dcs : co.drs) * elt;
+    const cudaError_t e =
+        to_device ? b200_h2d_2d(d, dpitch, h, hpitch, width, height, s)
+                  : cudaMemcpy2DAsync(h, hpitch, d, dpitch, width, height, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace
 
 int b200_colpipe_view_ok(long rows, long rs, long cs) {
@@ -491,9 +516,13 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
     if (has_in && e == cudaSuccess)
       e = b200_h2d_2d(in_dev, ci.dpitch, (const char *)p->in.host + ci.off * p->elt, ci.hpitch,
                       ci.width, ci.height, si);
-    if (e == cudaSuccess && p->out_read)
-      e = b200_h2d_2d(out_dev, co.dpitch, (const char *)p->out.host + co.off * p->elt, co.hpitch,
-                      co.width, co.height, si);
+    if (e == cudaSuccess && p->out_read) {
+      if (p->out_lower)
+        e = lower_panel_copy(p->out, j0, cols, p->elt, out_dev, co, true, si);
+      else
+        e = b200_h2d_2d(out_dev, co.dpitch, (const char *)p->out.host + co.off * p->elt,
+                        co.hpitch, co.width, co.height, si);
+    }
     if (e == cudaSuccess) e = cudaEventRecord(ev[q][0], si);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, ev[q][0], 0);
     if (e != cudaSuccess) {
@@ -506,8 +535,10 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
     e = cudaEventRecord(ev[q][1], sc);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(so, ev[q][1], 0);
     if (e == cudaSuccess)
-      e = cudaMemcpy2DAsync((char *)p->out.host + co.off * p->elt, co.hpitch, out_dev, co.dpitch,
-                            co.width, co.height, cudaMemcpyDeviceToHost, so);
+      e = p->out_lower ? lower_panel_copy(p->out, j0, cols, p->elt, out_dev, co, false, so)
+                       : cudaMemcpy2DAsync((char *)p->out.host + co.off * p->elt, co.hpitch,
+                                           out_dev, co.dpitch, co.width, co.height,
+                                           cudaMemcpyDeviceToHost, so);
     if (e == cudaSuccess) e = cudaEventRecord(ev[q][2], so);
     if (e != cudaSuccess) st = b200_set_error(B200_ECUDA, "pipeline: panel copy-out failed");
   }
