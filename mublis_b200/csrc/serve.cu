@@ -348,16 +348,18 @@ int mublis_b200_server_create(const mublis_b200_server_config_t *cfg, mublis_b20
       return b200_set_error(B200_ECUDA, "server: stream creation failed");
     }
   }
-  // Reserve scratch in the stream-ordered pool now (half the HBM budget, at
-  // most half of the free memory): a request's large scratch allocation that
-  // has to grow the pool maps new memory inside cudaMallocAsync, on the
-  // scheduler thread, which stalls every later dispatch (measured: up to
-  // 119 ms per allocation, a 2-3x loss of served throughput).  The pool keeps
-  // freed memory (its release threshold is raised at initialisation), so
-  // later allocations are carved from this reservation.
+  // Reserve the HBM budget in the stream-ordered pool now (at most half of
+  // the free memory): handles and request scratch are both carved from the
+  // pool, and admission keeps their sum within the budget, so the pool need
+  // not grow while serving.  Growing it maps new memory inside
+  // cudaMallocAsync, on the scheduler thread, which stalls every later
+  // dispatch (measured: up to 119 ms per allocation; with half the budget
+  // reserved and handles outside the pool, some runs of the served mix lost
+  // 2-3x of their throughput this way).  The pool keeps freed memory (its
+  // release threshold is raised at initialisation).
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-    const size_t reserve = std::min<size_t>(S->cfg.hbm_budget_bytes / 2, free_b / 2);
+    const size_t reserve = std::min<size_t>(S->cfg.hbm_budget_bytes, free_b / 2);
     void *p = nullptr;
     if (reserve > 0 && cudaMallocAsync(&p, reserve, S->streams[0]) == cudaSuccess)
       cudaFreeAsync(p, S->streams[0]);
@@ -379,11 +381,12 @@ int mublis_b200_server_destroy(mublis_b200_server_t *S) {
   }
   S->cv_work.notify_all();
   if (S->sched.joinable()) S->sched.join();
+  cudaDeviceSynchronize();
+  for (auto &h : S->handles) cudaFreeAsync(h.first, S->streams[0]);
   for (auto &s : S->streams) {
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
   }
-  for (auto &h : S->handles) cudaFree(h.first);
   delete S;
   return B200_OK;
 }
@@ -402,12 +405,15 @@ int mublis_b200_server_alloc(mublis_b200_server_t *S, size_t bytes, void **dptr)
       return b200_set_error(B200_ENOMEM, "server_alloc: HBM budget exceeded");
     S->hbm_handles += bytes;
   }
-  cudaError_t e = cudaMalloc(dptr, bytes ? bytes : 256);
+  // From the pool reserved at creation; usable on every stream once the
+  // allocating stream has synchronised.
+  cudaError_t e = cudaMallocAsync(dptr, bytes ? bytes : 256, S->streams[0]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S->streams[0]);
   std::lock_guard<std::mutex> lk(S->mu);
   if (e != cudaSuccess) {
     S->hbm_handles -= bytes;
     *dptr = nullptr;
-    return b200_set_error(B200_ENOMEM, "server_alloc: cudaMalloc failed");
+    return b200_set_error(B200_ENOMEM, "server_alloc: allocation failed");
   }
   S->handles[*dptr] = bytes;
   return B200_OK;
@@ -420,7 +426,10 @@ int mublis_b200_server_free(mublis_b200_server_t *S, void *dptr) {
   if (it == S->handles.end()) return b200_set_error(B200_EINVAL, "server_free: unknown handle");
   S->hbm_handles -= it->second;
   S->handles.erase(it);
-  cudaFree(dptr);
+  // The device-wide wait cudaFree implied: no queued work still reads it.
+  cudaDeviceSynchronize();
+  cudaFreeAsync(dptr, S->streams[0]);
+  cudaStreamSynchronize(S->streams[0]);
   return B200_OK;
 }
 
