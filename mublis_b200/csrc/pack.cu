@@ -143,37 +143,47 @@ __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long
 
 // General operands copied as stored (no structure, no domain mask, no
 // transform into planes): the plain forms' common case, without
-// pack_kernel's per-element structure checks.  A CTA moves 32 (mn) x 64
-// (kk) elements with eight loads in flight per thread; tiles wholly inside
-// the view skip the bounds checks.  Positive strides, mn_pad a multiple of
-// 32.  The panel is the one pack_kernel writes for the same view.
+// pack_kernel's per-element structure checks.  A CTA moves 32 (mn) x KT
+// (kk) elements with KT / 8 loads in flight per thread; tiles wholly
+// inside the view skip the bounds checks.  Positive strides, mn_pad a
+// multiple of 32.  The panel is the one pack_kernel writes for the same
+// view.
+constexpr int PACK_DENSE_KT = 128;
+
 template <typename T, bool MN_CONTIG>
 __global__ void __launch_bounds__(256)
     pack_dense_kernel(const T *__restrict__ x, long mn_stride, long kk_stride, long mn_len,
                       long k_len, long kk0, long kk1, PackOut o) {
-  __shared__ T tile[64][33];  // [kk_local][mn_local]
+  constexpr int KT = PACK_DENSE_KT, LOADS = KT / 8;
+  __shared__ T tile[KT][33];  // [kk_local][mn_local]
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const long mn_base = (long)blockIdx.x * 32;
-  const long kk_base = kk0 + (long)blockIdx.y * 64;
+  const long kk_base = kk0 + (long)blockIdx.y * KT;
   const long kend = kk1 < kk0 + k_len ? kk1 : kk0 + k_len;  // zeros from here on
-  const bool full = mn_base + 32 <= mn_len && kk_base + 64 <= kend;
+  const bool full = mn_base + 32 <= mn_len && kk_base + KT <= kend;
   const T *src = x + mn_base * mn_stride + (kk_base - kk0) * kk_stride;
+  T val[LOADS];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
+  for (int q = 0; q < LOADS; ++q) {
     // Lanes run along the source's unit-stride dimension.
     const int mn_l = MN_CONTIG ? tx : ty + 8 * (q & 3);
     const int kk_l = MN_CONTIG ? ty + 8 * q : tx + 32 * (q >> 2);
-    T val = T(0);
+    val[q] = T(0);
     if (full || (mn_base + mn_l < mn_len && kk_base + kk_l < kend))
-      val = src[mn_l * mn_stride + kk_l * kk_stride];
-    tile[kk_l][mn_l] = val;
+      val[q] = src[mn_l * mn_stride + kk_l * kk_stride];
+  }
+#pragma unroll
+  for (int q = 0; q < LOADS; ++q) {
+    const int mn_l = MN_CONTIG ? tx : ty + 8 * (q & 3);
+    const int kk_l = MN_CONTIG ? ty + 8 * q : tx + 32 * (q >> 2);
+    tile[kk_l][mn_l] = val[q];
   }
   __syncthreads();
   if (o.layout == PACK_FRAG64) {
     if constexpr (sizeof(T) == 8) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int combo = ty + 8 * q;  // 2 blocks of 16 rows x 16 k-quads
+      for (int q = 0; q < KT / 16; ++q) {
+        const int combo = ty + 8 * q;  // 2 blocks of 16 rows x KT / 4 k-quads
         const int mn_l = (combo & 1) * 16 + (tx >> 2), kk_l = (combo >> 1) * 4 + (tx & 3);
         const long kk = kk_base + kk_l;
         if (kk >= kk1) continue;
@@ -186,7 +196,7 @@ __global__ void __launch_bounds__(256)
   }
   T *out = (T *)o.out + mn_base + tx;  // PACK_MN_MAJOR
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
+  for (int q = 0; q < LOADS; ++q) {
     const int kk_l = ty + 8 * q;
     const long kk = kk_base + kk_l;
     if (kk < kk1) out[kk * o.ld] = tile[kk_l][tx];
@@ -533,7 +543,8 @@ int launch_pack(const PackView &v, bool b_side, long mn_len, long k_len, long mn
                           mn_pad % 32 == 0 &&
                           (o.layout == PACK_MN_MAJOR || (o.layout == PACK_FRAG64 && sizeof(T) == 8));
   if (plain_copy) {
-    dim3 grid((unsigned)b200_ceil_div(mn_pad, 32), (unsigned)b200_ceil_div(kk1 - kk0, 64));
+    dim3 grid((unsigned)b200_ceil_div(mn_pad, 32),
+              (unsigned)b200_ceil_div(kk1 - kk0, PACK_DENSE_KT));
     if (grid.y > 65535) return b200_set_error(B200_EINVAL, "pack: k extent too large");
     const T *x = (const T *)v.x;
     if (mn_fast)
