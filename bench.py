@@ -20,10 +20,12 @@ those 18 calls through the cblas_* entry points.
   (library profiler, recorded on the launching stream during the timed
   region) against its pipe's peak.
 * cpu_baseline: the reference's own avx2 build (oracle/_ref) on the host
-  cores, run on a bounded sample (the same family at n = 2048, one pass
-  per host thread, all threads concurrently).
-* --impl reference: the reference's avx2 build timed on the same family
-  (n = 1024 per step, every host thread a concurrent caller).
+  cores: one step of the same n = 4096 family, every call cut into column
+  panels that are separate reference calls, spread over all host threads
+  (the library is single-threaded per call); plus the family at n = 2048
+  on one thread.
+* --impl reference: the reference's avx2 build timed the same way on the
+  same n = 4096 family, --steps timed steps after --warmup untimed ones.
 
 Multi-GPU: the path does not shard (one BLAS call per GPU); --gpus N runs N
 independent replicas under torchrun, value = total flops / max-over-ranks
@@ -164,14 +166,22 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- reference arm
 
-def ref_bench(n: int, threads: int, reps: int, warmup: int) -> dict:
+def ref_bench(n: int, threads: int, reps: int, warmup: int, mode: str = "family",
+              panel: int = 512) -> dict:
+    """Times the reference's own avx2 build through oracle/lib/ref_bench.
+    mode "family": every thread runs the whole 18-call family on its own
+    operands; "family_par": one shared family of 18 calls, each cut into
+    column panels of `panel` columns (separate reference cblas calls), spread
+    over all threads, one pass per step."""
     from oracle import oracle as orc  # checker/baseline only
     lib = orc.ref_lib_path("avx2")
     if not lib.is_file() or not orc.REF_BENCH.is_file():
         raise FileNotFoundError("reference build missing (make -C oracle)")
-    out = subprocess.run([str(orc.REF_BENCH), str(lib), "family", "x", str(n), str(n), str(n),
-                          str(threads), str(reps), str(warmup)], check=True,
-                         capture_output=True, text=True).stdout
+    cmd = [str(orc.REF_BENCH), str(lib), mode, "x", str(n), str(n), str(n), str(threads),
+           str(reps), str(warmup)]
+    if mode == "family_par":
+        cmd.append(str(panel))
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     return json.loads(out.strip().splitlines()[-1])
 
 
@@ -182,28 +192,33 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def par_sample(n: int, threads: int, panel: int) -> str:
+    return (f"per step: the 18-call family at m=n=k={n} (the benchmarked workload), every call "
+            f"cut into column panels of {panel} columns issued as separate reference cblas "
+            f"calls (SYRK/SYR2K: diagonal block + GEMMs below), largest first over {threads} "
+            f"host threads (reference linux_avx2 build, 1 thread per call)")
+
+
 def run_reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    n = 1024
+    n = args.n
     threads = host_threads()
-    config = workload_config(args.n)
+    config = workload_config(n)
     try:
-        r = ref_bench(n, threads, args.steps, args.warmup)
+        r = ref_bench(n, threads, args.steps, args.warmup, mode="family_par", panel=512)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference build not runnable: {e}"}))
         return
     ms = r["wall_s"] / args.steps * 1e3
     value = r["gflops_aggregate"] / 1e3
-    sample = (f"per step: the 18-call family at m=n=k={n} issued by each of {threads} host "
-              f"threads concurrently (reference linux_avx2 build, 1 thread per call)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic", "config": config,
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": par_sample(n, threads, 512)},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))
 
@@ -303,6 +318,67 @@ class Family:
                                               n, ptr[1], n)
 
 
+def verify_step(torch, fam, ncheck: int = 16, seed: int = 7) -> dict:
+    """Checks one more step of the family, outside the timed region: on
+    `ncheck` seeded columns of every call's output, the normwise error against
+    a float64 evaluation of the same columns on the device (torch; TRSM by a
+    float64 triangular solve, relative forward error), divided by the stated
+    bound 4*k*u.  SYRK/SYR2K's upper triangle must come back unchanged."""
+    n = fam.n
+    g = torch.Generator().manual_seed(seed)
+    cols = torch.randperm(n, generator=g)[:ncheck].sort().values.cuda()
+    norm = torch.linalg.norm
+    before = []
+    for p, r, ops in fam.calls:
+        out = ops[1] if r in ("trmm", "trsm") else ops[2]
+        before.append(out.t()[:, cols].to(torch.float64))
+    fam.step()
+    torch.cuda.synchronize()
+    worst, untouched, per_call = 0.0, True, {}
+    rows = torch.arange(n, device="cuda").unsqueeze(1)
+    lower = rows >= cols.unsqueeze(0)
+    for (p, r, ops), c0 in zip(fam.calls, before):
+        u = 2.0 ** -24 if p == "s" else 2.0 ** -53
+        A = ops[0].t().to(torch.float64)
+        k = 2 * n if r == "syr2k" else n
+        if r in ("trmm", "trsm"):
+            L = torch.tril(A)
+            got = ops[1].t()[:, cols].to(torch.float64)
+            if r == "trmm":
+                ref = ALPHA * (L @ c0)
+                err = norm(got - ref) / (ALPHA * norm(L) * norm(c0))
+            else:
+                ref = torch.linalg.solve_triangular(L, ALPHA * c0, upper=False)
+                err = norm(got - ref) / norm(ref)
+        else:
+            B = ops[1].t().to(torch.float64)
+            got = ops[2].t()[:, cols].to(torch.float64)
+            if r.startswith("gemm"):
+                opa = A.t() if r[5] == "t" else A
+                opb = (B.t() if r[6] == "t" else B)[:, cols]
+                prod, fa = opa @ opb, norm(opa) * norm(opb)
+            elif r == "symm":
+                sym = torch.tril(A) + torch.tril(A, -1).t()
+                prod, fa = sym @ B[:, cols], norm(sym) * norm(B[:, cols])
+            elif r == "syrk":
+                prod, fa = A @ A[cols, :].t(), norm(A) * norm(A[cols, :])
+            else:
+                prod = A @ B[cols, :].t() + B @ A[cols, :].t()
+                fa = norm(A) * norm(B[cols, :]) + norm(B) * norm(A[cols, :])
+            ref = ALPHA * prod + BETA * c0
+            if r in ("syrk", "syr2k"):
+                untouched = untouched and bool(torch.equal(got[~lower], c0[~lower]))
+                got, ref, c0 = got * lower, ref * lower, c0 * lower
+            err = norm(got - ref) / (ALPHA * fa + BETA * norm(c0))
+        ratio = float(err) / (4 * k * u)
+        per_call[f"{p}{r}"] = round(ratio, 6)
+        worst = max(worst, ratio)
+    return {"calls": len(fam.calls), "columns_per_call": ncheck,
+            "max_err_over_bound": round(worst, 6), "bound": "4*k*u normwise (TRSM: relative "
+            "forward error 4*n*u)", "upper_triangle_untouched": untouched,
+            "err_over_bound": per_call}
+
+
 def timed(torch, fn, steps: int):
     s = torch.cuda.current_stream()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -316,9 +392,12 @@ def timed(torch, fn, steps: int):
     return e0.elapsed_time(e1) / steps
 
 
+FORM_CALLS = 10  # timed calls per form in the 8192 study (mean of one event pair)
+
+
 def forms_study(torch, lib, n: int = 8192) -> dict:
-    """Precision forms at m = n = k = n (8192 by default; one call each,
-    event-timed)."""
+    """Precision forms at m = n = k = n (8192 by default): one warm-up call,
+    then FORM_CALLS back-to-back calls timed by one CUDA-event pair."""
     out = {}
     for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6", "fp16x3", "ozaki2"]),
                          ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
@@ -333,7 +412,7 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
                               ctypes.c_void_p(b.data_ptr()), n, 0.5,
                               ctypes.c_void_p(c.data_ptr()), n)
             call()
-            ms = timed(torch, call, 2)
+            ms = timed(torch, call, FORM_CALLS)
             out[f"{p}gemm_{n}_{f}"] = round(2.0 * n ** 3 / ms / 1e9, 2)
         lib.mublis_b200_set_form(p.encode(), b"plain")
         del a, b, c
@@ -358,7 +437,7 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
                                        ctypes.c_void_p(b.data_ptr()), n)
         call()
         b.copy_(b0)
-        ms = timed(torch, call, 2)
+        ms = timed(torch, call, FORM_CALLS)
         b.copy_(b0)
         out[f"dtrsm_{n}_{f}"] = round(float(n) ** 3 / ms / 1e9, 2)
     lib.mublis_b200_set_form(b"d", b"plain")
@@ -721,6 +800,10 @@ def main():
             t1 = timed(torch, single.step, 1)
             breakdown[f"{p}{r}"] = round(flops(r, n) / (t1 * 1e-3) / 1e12, 2)
 
+    verified = None
+    if rank == 0 and not args.only_timed:
+        verified = verify_step(torch, fam)
+
     # roofline of the dominant kernel
     roof = None
     if kstats and rank == 0:
@@ -771,7 +854,9 @@ def main():
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
+        fsampler = ClockSampler(gpu_index)
         forms = forms_study(torch, lib, args.forms_n)
+        forms["clocks"] = fsampler.stop()
     grouped = served = None
     if rank == 0 and world == 1 and not args.no_studies:
         grouped = grouped_study(torch, lib)
@@ -781,17 +866,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             threads = host_threads()
-            r = ref_bench(2048, threads, 1, 0)
+            r = ref_bench(n, threads, 1, 0, mode="family_par", panel=512)
             r1 = ref_bench(2048, 1, 1, 0)  # one call at a time on one core
             cpu = {"value": round(r["gflops_aggregate"] / 1e3, 4), "unit": "TFLOP/s",
                    "cores": threads, "kind": "reference",
-                   "sample": f"the 18-call family at m=n=k=2048, one pass per host thread, "
-                             f"{threads} threads concurrently, reference linux_avx2 build "
-                             f"(oracle/_ref), wall {r['wall_s']:.1f} s",
+                   "sample": par_sample(n, threads, 512) + f"; one step, wall {r['wall_s']:.1f} s",
                    "one_thread": {"value": round(r1["gflops_aggregate"] / 1e3, 4),
                                   "unit": "TFLOP/s", "cores": 1,
-                                  "sample": f"the same family, one pass on one thread, "
-                                            f"wall {r1['wall_s']:.1f} s"}}
+                                  "sample": f"the 18-call family at m=n=k=2048, one pass on one "
+                                            f"thread, wall {r1['wall_s']:.1f} s"}}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unavailable": str(e)}
 
@@ -803,9 +886,10 @@ def main():
                 "A off-diagonal uniform/n, diagonal uniform[1,2)",
                 "config": workload_config(n), "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clocks, "gpu_launches": int(launches), "breakdown_tflops": breakdown,
+                "verified": verified,
                 "stated_err": "normwise relative error <= 4*k*u against the oracle "
-                              "(tests/test_gpu_parity.py); measured plain SGEMM ~1.9e-8, "
-                              "DGEMM ~3.4e-17 at 8192 (profiles/precision_forms_8192.md)",
+                              "(tests/test_gpu_config2.py checks this workload's 18 calls); "
+                              "measured plain SGEMM ~1.9e-8, DGEMM ~3.4e-17 at 8192",
                 "forms_8192_tflops": forms, "grouped_config4": grouped, "served_config5": served,
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in kstats.items()}}
         print(json.dumps(line))

@@ -56,6 +56,15 @@ unsigned long long mublis_b200_launch_count(void);
 int mublis_b200_profile_enable(int on);
 int mublis_b200_profile_read(char *buf, unsigned long len);
 
+/* Failure-detection test of the bounded device waits.  Arms a one-shot
+ * stall for the next launch of the FP64 tensor-pipe GEMM kernel in the
+ * process: that launch bounds its mbarrier waits by wait_limit_ns (at most
+ * 2 s) instead of 2 s, and its producer issues no loads, so the consumers'
+ * first wait runs out; the kernel raises its abort flag and error word and
+ * returns (nothing faults, nothing spins unbounded), and the call that made
+ * the launch returns 4.  Later launches run normally. */
+int mublis_b200_test_stall_next(unsigned long long wait_limit_ns);
+
 /* Seeded device fills (Philox4x32-10, key = (seed, matrix_id), counter =
  * column-major element index i + j*m; kind 0 uniform[-1,1), 1 wide
  * +-[1,2)*2^[-10,10], 2 uniform[1,2)).  x is a device pointer to an m x n
@@ -175,19 +184,25 @@ int mublis_b200_server_reset_stats(mublis_b200_server_t *srv);
  * For callers that cannot allocate device memory when they call in: a
  * process whose GPU memory is already owned by another allocator, or a
  * service that keeps a fixed device footprint and bans cudaMalloc/cudaFree
- * on its request path.  Same arguments and result as mublis_sgemm, but A, B
- * and C must be device pointers (staging host buffers would allocate), and
- * the packed operand panels live in a fixed 32 MiB scratch array that is
- * part of the library's device image, held on every GPU that loads the
- * library until the process exits.  Limit:
+ * on its request path.  Same arguments, checks and result as mublis_sgemm
+ * with the plain FP32 kernel (the form chosen by MUBLIS_B200_SFORM or
+ * mublis_b200_set_form does not apply here), but A, B and C must be device
+ * pointers (staging host buffers would allocate), and the packed operand
+ * panels live in a fixed 32 MiB scratch array in the library's device code.
+ * Limit:
  *   (roundup(m, 128) + roundup(n, 128)) * roundup(k, 16) <= 8388608 floats
  * (e.g. m = n = k = 2048); larger sizes return 1 with a message in
  * mublis_b200_last_error() and leave C untouched.
- * The first call on each device resolves the array's device address
- * (cudaGetSymbolAddress with that device current); make that first call
- * before any stream capture.  All calls on a device share the array and it
- * keeps the last call's contents (nothing in it needs to start at zero);
- * calls that overlap on the GPU race on it, so do not overlap them. */
+ * The array is claimed once per device: on the device current when the
+ * library initialises (mublis_b200_init, or the first call of any entry
+ * point), at that point; on any other device, by the first call of this
+ * function there, which looks up the array's device address with that
+ * device current -- make that first call before any stream capture.  The
+ * device keeps the array until the process exits.  All calls on a device
+ * share it and it keeps the last call's contents (nothing in it needs to
+ * start at zero); calls that overlap on the GPU race on it, so do not
+ * overlap them.  Like the other entry points, it returns after
+ * synchronizing the calling thread's library stream. */
 int mublis_b200_sgemm_noalloc(mublis_trans_t trans_a, mublis_trans_t trans_b, int m, int n, int k,
                               float alpha, const float *a, int rs_a, int cs_a, const float *b,
                               int rs_b, int cs_b, float beta, float *c, int rs_c, int cs_c);

@@ -118,6 +118,7 @@ EXTENSIONS = {
     "mublis_b200_launch_count": ([], ctypes.c_ulonglong),
     "mublis_b200_profile_enable": ([_I], _I),
     "mublis_b200_profile_read": ([ctypes.c_char_p, ctypes.c_ulong], _I),
+    "mublis_b200_test_stall_next": ([ctypes.c_ulonglong], _I),
     "mublis_b200_fill_s": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_b200_fill_d": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_get_context": ([_P], _I),

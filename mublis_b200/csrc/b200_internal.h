@@ -184,6 +184,15 @@ int b200_copy_h2d(void *dst, long ld, const void *src, long rs, long cs, long ro
 int b200_copy_d2h(void *dst, long rs, long cs, const void *src, long ld, long rows, long cols,
                   size_t elt);
 
+/* runtime.cu: the wait limit armed by mublis_b200_test_stall_next (0 when
+ * none is armed), cleared by the call: the next FP64 tensor-pipe GEMM launch
+ * takes it and stalls. */
+unsigned long long b200_take_test_stall(void);
+
+/* noalloc.cu: resolves the allocation-free SGEMM's fixed scratch array on
+ * the current device (run once by b200_init). */
+void b200_noalloc_setup(void);
+
 /* tc_gemm.cu: nonzero (and cleared) if a kernel reported a bounded-wait
  * timeout since the last call. */
 int b200_take_device_error(void);

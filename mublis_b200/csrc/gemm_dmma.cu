@@ -102,7 +102,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   if (warp == CONSUMERS) {
     // ---------------- producer ----------------
-    if (lane != 0) return;
+    // A stalled launch (armed by mublis_b200_test_stall_next) issues nothing:
+    // the consumers' first bounded wait runs out, they raise the abort flag
+    // and the error word, and the launch ends with status 4 on the host.
+    if (lane != 0 || p.stall) return;
     int stage = 0, issued = 0;
     uint32_t phase = 0;
     bool ok = true;
@@ -113,7 +116,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       const double *ga = p.ap + (long)tm * p.kq * 2 * 8 * 32;
       const double *gb = p.bp + (long)tn * p.kq * 2 * 8 * 32;
       for (int kt = kt0; kt < kt1; ++kt) {
-        if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err, p.wait_ns)) {
+          ok = false;
+          break;
+        }
         tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
         unsigned char *dst = smem + stage * STAGE_BYTES;
         tc::bulk_load_1d(dst, ga + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES, &full[stage]);
@@ -148,7 +154,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
     for (int kt = kt0; kt < kt1; ++kt) {
-      const int wok = tc::mbar_wait(&full[stage], phase, abort_flag, p.err);
+      const int wok = tc::mbar_wait(&full[stage], phase, abort_flag, p.err, p.wait_ns);
       if (!__all_sync(0xffffffffu, wok)) return;
       const double2 *As = (const double2 *)(smem + stage * STAGE_BYTES) + wm * 4 * 32 + lane;
       const double2 *Bs =

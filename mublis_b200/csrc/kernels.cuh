@@ -155,6 +155,8 @@ struct DmmaGemmArgs {
   double alpha, beta;
   int jp, ji, pi;
   int *err;
+  unsigned long long wait_ns;  // bound of every mbarrier wait
+  int stall;                   // failure-detection test: the producer issues no loads
 };
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s);
 constexpr int B200_DMMA_TILE = 128, B200_DMMA_BK = 16;

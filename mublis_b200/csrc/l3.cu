@@ -159,6 +159,12 @@ int run_dmma(const b200_l3_desc_t *d) {
     g.ji = d->product.domain.ji;
     g.pi = d->product.domain.pi;
     g.err = b200_device_error_word();
+    g.wait_ns = B200_WAIT_NS;
+    g.stall = 0;
+    if (const unsigned long long limit = b200_take_test_stall()) {
+      g.wait_ns = limit;
+      g.stall = 1;
+    }
     st = launch_dmma_gemm(g, s);
   }
   b200_free(list);

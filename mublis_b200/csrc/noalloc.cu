@@ -12,11 +12,16 @@
 // memory allocated per call.
 //
 // The array, g_noalloc_scratch, holds NOALLOC_SCRATCH_FLOATS floats
-// (32 MiB).  Every GPU on which the library's device code is loaded keeps it
-// until the process exits.  In host code its name is only a host-side
-// stand-in for the device symbol, so the device address is obtained once
-// per device, with that device current, through cudaGetSymbolAddress; the
-// first call on each device performs that set-up.
+// (32 MiB).  In host code its name is only a host-side stand-in for the
+// device symbol, so the device address is obtained once per device, with
+// that device current, through cudaGetSymbolAddress.  That lookup is also
+// what loads this file's device code (CUDA loads modules lazily) and with it
+// claims the 32 MiB, which the device then keeps until the process exits.
+// The library's initialisation (b200_init, run by mublis_b200_init or the
+// first call of any entry point) does it for the device current at that
+// moment, so the memory is claimed when the library starts, not on a
+// request path; on any other device the first call of this entry point
+// there does it.
 //
 // Every call on a device shares the one array, and the array keeps whatever
 // the last call left in it.  Nothing in it needs to start at zero: the pack
@@ -42,8 +47,8 @@ float *g_scratch_addr[NOALLOC_MAX_DEVICES];
 int g_scratch_status[NOALLOC_MAX_DEVICES];
 std::once_flag g_scratch_once[NOALLOC_MAX_DEVICES];
 
-// Device address of g_noalloc_scratch on the current device (set up on the
-// first call for that device).
+// Device address of g_noalloc_scratch on the current device (looked up
+// once per device).
 int scratch_on_current_device(float **out) {
   int dev = 0;
   B200_CUDA_TRY(cudaGetDevice(&dev));
@@ -69,12 +74,23 @@ int scratch_on_current_device(float **out) {
 
 }  // namespace
 
+// Called once by the library's initialisation with the device it brings up
+// current: resolves (and so claims) the scratch array there.  A failure is
+// kept and reported by the entry point's first call; it does not fail the
+// initialisation of everything else.
+extern "C" void b200_noalloc_setup(void) {
+  float *unused = nullptr;
+  (void)scratch_on_current_device(&unused);
+}
+
 extern "C" int mublis_b200_sgemm_noalloc(mublis_trans_t trans_a, mublis_trans_t trans_b, int m,
                                          int n, int k, float alpha, const float *a, int rs_a,
                                          int cs_a, const float *b, int rs_b, int cs_b, float beta,
                                          float *c, int rs_c, int cs_c) {
-  if (m < 0 || n < 0 || k < 0) return b200_set_error(B200_EINVAL, "sgemm_noalloc: negative size");
+  // Same order of checks as mublis_sgemm: an empty output returns before
+  // the sizes are checked.
   if (m == 0 || n == 0) return B200_OK;
+  if (m < 0 || n < 0 || k < 0) return b200_set_error(B200_EINVAL, "sgemm_noalloc: negative size");
   B200_TRY(b200_init());
   const bool update = alpha != 0.f && k > 0;
   if (!b200_is_device_ptr(c) || (update && (!b200_is_device_ptr(a) || !b200_is_device_ptr(b))))

@@ -78,6 +78,9 @@ void do_init() {
   if (sslices > 0) g_default_slices[B200_F32] = sslices;
   g_init_status = B200_OK;
   b200_tune_autoload();
+  // The allocation-free SGEMM's fixed scratch array is claimed here, at
+  // start-up, rather than on that entry point's first call.
+  b200_noalloc_setup();
 }
 
 }  // namespace
@@ -196,6 +199,20 @@ int b200_alloc(void **p, size_t bytes) {
 void b200_free(void *p) {
   if (p) cudaFreeAsync(p, b200_cur_stream());
 }
+
+namespace {
+std::atomic<unsigned long long> g_test_stall{0};
+constexpr unsigned long long B200_TEST_STALL_MAX_NS = 2000000000ull;
+}  // namespace
+
+int mublis_b200_test_stall_next(unsigned long long wait_limit_ns) {
+  if (wait_limit_ns == 0 || wait_limit_ns > B200_TEST_STALL_MAX_NS)
+    return b200_set_error(B200_EINVAL, "test_stall_next: limit must be in (0, 2 s]");
+  g_test_stall.store(wait_limit_ns);
+  return B200_OK;
+}
+
+unsigned long long b200_take_test_stall(void) { return g_test_stall.exchange(0); }
 
 int b200_set_error(int code, const char *where) {
   snprintf(t_error, sizeof t_error, "%s", where);

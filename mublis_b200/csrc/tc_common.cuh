@@ -63,15 +63,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase of parity `parity` to complete.
+// Bounded wait for the phase of parity `parity` to complete, for at most
+// limit_ns.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                          int *err) {
+                                          int *err, uint64_t limit_ns = B200_WAIT_NS) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (globaltimer() - t0 > B200_WAIT_NS) {
+    if (globaltimer() - t0 > limit_ns) {
       *abort_flag = 1;
       if (err) atomicExch(err, B200_ETIMEOUT);
       return false;

@@ -5,8 +5,11 @@ restatement, or against a double-double evaluation of sampled entries at
 8192^3):
   plain FP32 / FP64     4 * k * u                      (u = 2^-24 / 2^-53)
   bf16x6 (FP32)         4 * k * 2^-24                  (same as plain)
-  bf16x3 (FP32)         2^-15   (16-bit split of each input: ~2^-17 per
-                                 element, not k-dependent)
+  bf16x3 (FP32)         2^-19   (the split keeps 16 bits of each input,
+                                 |x - hi - lo| <= 2^-18 |x|; the error is
+                                 not k-dependent, ~2^-18 / sqrt(k) normwise
+                                 for random signs); at 8192^3 at most 4x
+                                 plain FP32's measured error
   fp16x3 (FP32)         4 * k * 2^-24  (scaled fp16 split: ~24-bit inputs)
   ozaki:8 (FP64)        4 * k * 2^-53                  (same as plain)
   ozaki:7 (FP64)        2^-44
@@ -34,7 +37,7 @@ TOL = {
     "plain": lambda k, u: 4 * k * u,
     "bf16x6": lambda k, u: 4 * k * 2.0 ** -24,
     "fp16x3": lambda k, u: 4 * k * 2.0 ** -24,
-    "bf16x3": lambda k, u: 2.0 ** -15,
+    "bf16x3": lambda k, u: 2.0 ** -19,
     "ozaki:8": lambda k, u: 4 * k * 2.0 ** -53,
     "ozaki:7": lambda k, u: 2.0 ** -44,
     "ozaki2": lambda k, u: 4 * k * u,
@@ -269,7 +272,7 @@ def test_precision_study_8192(lib, kind):
     assert table["dgemm ozaki2"][0] <= table["dgemm plain"][0]
     assert table["sgemm ozaki2"][0] <= table["sgemm plain"][0]
     assert table["sgemm fp16x3"][0] <= table["sgemm plain"][0]
-    assert table["sgemm bf16x3"][0] <= TOL["bf16x3"](n, 0)
+    assert table["sgemm bf16x3"][0] <= 4 * table["sgemm plain"][0]
     assert table["dgemm ozaki:7"][0] <= TOL["ozaki:7"](n, 0)
 
 

@@ -205,11 +205,43 @@ def test_general_strides(lib, p):
     assert err <= 4 * k * cs.EPS[np.dtype(dt)]
 
 
+# The generic driver's whole case matrix: every (jp, ji, pi) relation triple
+# (ALL / LOWER / UPPER each) with every operand structure (GENERAL,
+# SYMMETRIC, TRIANGULAR) for A and for B.  The stored triangle of a
+# structured operand and a triangular operand's unit diagonal alternate with
+# the case index, so both triangles and both diagonal treatments occur.
+def _driver_matrix():
+    out = []
+    for idx, (jp, ji, pi, sa, sb) in enumerate(itertools.product(range(3), range(3), range(3),
+                                                                 range(3), range(3))):
+        def operand(struc, salt):
+            if struc == 0:
+                return (0, 0, 0)
+            uplo = 1 + (idx + salt) % 2
+            diag = (idx // 2 + salt) % 2 if struc == 2 else 0
+            return (struc, uplo, diag)
+        out.append(dict(jp=jp, ji=ji, pi=pi, a=operand(sa, 0), b=operand(sb, 1)))
+    return out
+
+
+DRIVER_MATRIX = _driver_matrix()
+
+
+def _driver_id(dc):
+    names = "AlU"
+    s = "GST"
+    return (f"jp{names[dc['jp']]}-ji{names[dc['ji']]}-pi{names[dc['pi']]}-"
+            f"a{s[dc['a'][0]]}{dc['a'][1]}{dc['a'][2]}-b{s[dc['b'][0]]}{dc['b'][1]}{dc['b'][2]}")
+
+
 @pytest.mark.parametrize("p", ["s", "d"])
-@pytest.mark.parametrize("dc_idx", range(5))
-def test_generic_driver_domains(lib, p, dc_idx):
-    from tests.test_oracle_pins import DRIVER_CASES
-    dc = DRIVER_CASES[dc_idx]
+@pytest.mark.parametrize("dc", DRIVER_MATRIX, ids=[_driver_id(d) for d in DRIVER_MATRIX])
+def test_generic_driver_domains(lib, p, dc):
+    """mublis_l3_{s,d}driver on the device against the oracle's driver
+    (element-wise domain semantics of l3_driver.c:49-256 and packm.c:40-71)
+    for every domain relation triple and operand structure; the unstored
+    triangles and unit diagonals are NaN.  Normwise error <= 4 k u and the
+    part of C outside ji bit-identical to its input."""
     dt = np.float32 if p == "s" else np.float64
     m = n = k = 161
     a = orc.fill(m, k, dt, 3, 0)
@@ -233,6 +265,9 @@ def test_generic_driver_domains(lib, p, dc_idx):
     err = np.linalg.norm(outs[0] - outs[1]) / (fa + 0.25 * np.linalg.norm(c0))
     assert np.isfinite(outs[1]).all()
     assert err <= 4 * k * cs.EPS[np.dtype(dt)]
+    i, j = np.indices((m, n))
+    outside = (j > i) if dc["ji"] == 1 else (j < i) if dc["ji"] == 2 else np.zeros((m, n), bool)
+    np.testing.assert_array_equal(outs[1][outside], c0[outside])
 
 
 def test_device_pointers_in_place(lib):

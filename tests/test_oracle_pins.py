@@ -159,3 +159,25 @@ def test_restated_driver_matches_reference_driver(dc, p):
     err = np.linalg.norm(np.nan_to_num(outs[0] - outs[1])) / (fa + 0.25 * np.linalg.norm(c0))
     assert np.isfinite(outs[0]).all() and np.isfinite(outs[1]).all()
     assert err <= tol
+
+
+@pytest.mark.parametrize("n,panel", [(300, 64), (257, 100)])
+def test_parallel_reference_family_panels_match_whole_calls(n, panel):
+    """The benchmark's reference arm cuts every call of the family into
+    column panels issued as separate reference calls (SYRK/SYR2K: a
+    diagonal-block SYRK/SYR2K plus GEMMs below it) to use every host thread.
+    Its check mode recomputes each call whole on the same inputs: the panels
+    must give the same result up to rounding (a wrong cut would differ by
+    O(1))."""
+    import json
+    import subprocess
+    lib = orc.ref_lib_path("avx2")
+    if not lib.is_file() or not orc.REF_BENCH.is_file():
+        pytest.skip("reference build not present")
+    out = subprocess.run([str(orc.REF_BENCH), str(lib), "family_par", "x", str(n), str(n),
+                          str(n), "4", "1", "0", str(-panel)], check=True, capture_output=True,
+                         text=True).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    assert r["routine"] == "family_par_check"
+    assert r["tasks"] == 18 * -(-n // panel)
+    assert r["max_rel_diff"] <= 1e-5, r
