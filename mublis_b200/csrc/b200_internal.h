@@ -97,6 +97,18 @@ typedef struct {
 int b200_trsm_prepare(const b200_trsm_desc_t *d, void **prep);
 void b200_trsm_release(void *prep);
 
+/* trsm_leaf.cu: the fused GEMMTRSM kernel on leaves of b200_trsm_leaf_rows()
+ * rows.  pack: every leaf of op(A) (order m; lower, or upper read reversed)
+ * into leaves * b200_trsm_leaf_stride() elements; solve: one leaf of `rows`
+ * rows for n right-hand sides, b at the leaf's first row in lower
+ * orientation (an upper leaf: its last row, rs_b negated). */
+long b200_trsm_leaf_rows(void);
+long b200_trsm_leaf_stride(void);
+int b200_trsm_leaf_pack(int dtype, const void *a, long rs_a, long cs_a, int m, int lower,
+                        int unit, void *out);
+int b200_trsm_leaf_solve(int dtype, const void *pack, int rows, void *b, long rs_b, long cs_b,
+                         int n);
+
 /* runtime.cu */
 int b200_init(void);
 int b200_device_count(void);

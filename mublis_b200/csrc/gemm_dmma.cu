@@ -82,6 +82,15 @@ __device__ __forceinline__ bool tile_krange(const DmmaGemmArgs &p, int tm, int t
   return true;
 }
 
+// Chunk `chunk` of S of the k-blocks [kt0, kt1) (depends only on the
+// tile's k range and S).
+__device__ __forceinline__ void chunk_range(int chunk, int S, int &kt0, int &kt1) {
+  const int per = (kt1 - kt0 + S - 1) / S;
+  const int b = min(kt1, kt0 + chunk * per);
+  kt1 = min(kt1, b + per);
+  kt0 = b;
+}
+
 __global__ void __launch_bounds__(THREADS, 1)
     dmma_gemm_kernel(const __grid_constant__ DmmaGemmArgs p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -99,6 +108,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
   __syncthreads();
   const int num_tiles = p.tile_list ? p.ntiles : p.tiles_m * p.tiles_n;
+  const int S = p.splits;
+  const int num_units = num_tiles * S;
 
   if (warp == CONSUMERS) {
     // ---------------- producer ----------------
@@ -109,10 +120,11 @@ __global__ void __launch_bounds__(THREADS, 1)
     int stage = 0, issued = 0;
     uint32_t phase = 0;
     bool ok = true;
-    for (int idx = blockIdx.x; idx < num_tiles && ok; idx += gridDim.x) {
+    for (int u = blockIdx.x; u < num_units && ok; u += gridDim.x) {
       int tm, tn, kt0, kt1;
-      tile_coords(p, idx, tm, tn);
+      tile_coords(p, u / S, tm, tn);
       if (!tile_krange(p, tm, tn, kt0, kt1)) continue;
+      chunk_range(u % S, S, kt0, kt1);
       const double *ga = p.ap + (long)tm * p.kq * 2 * 8 * 32;
       const double *gb = p.bp + (long)tn * p.kq * 2 * 8 * 32;
       for (int kt = kt0; kt < kt1; ++kt) {
@@ -142,10 +154,11 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int g = lane >> 2, t = lane & 3;
   int stage = 0;
   uint32_t phase = 0;
-  for (int idx = blockIdx.x; idx < num_tiles; idx += gridDim.x) {
+  for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
     int tm, tn, kt0, kt1;
-    tile_coords(p, idx, tm, tn);
+    tile_coords(p, u / S, tm, tn);
     if (!tile_krange(p, tm, tn, kt0, kt1)) continue;
+    chunk_range(u % S, S, kt0, kt1);
     double acc[4][4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -175,6 +188,42 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&empty[stage]);
       if (++stage == STAGES) { stage = 0; phase ^= 1; }
+    }
+
+    // Split-K: each warp stores its 64 x 32 sums of this chunk (element e of
+    // lane l at e * 256 + 32 warp + l: 256 contiguous bytes per warp store);
+    // the warp that finishes its sub-tile's last chunk (a per-(tile, warp)
+    // counter -- no block-wide barrier, so a warp never waits on another)
+    // adds the S chunks' sums in chunk order and runs the epilogue.
+    if (S > 1) {
+      const int slot = threadIdx.x;  // consumer thread 0..255
+      double *mine = p.partials + (size_t)u * 64 * 256;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) mine[((i * 4 + j) * 4 + e) * 256 + slot] = acc[i][j][e];
+      __threadfence();
+      __syncwarp();
+      int last = 0;
+      if (lane == 0) last = atomicAdd(&p.arrivals[(u / S) * CONSUMERS + warp], 1) == S - 1;
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (!last) continue;
+      __threadfence();
+      const double *first = p.partials + (size_t)(u / S) * S * 64 * 256;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int off = ((i * 4 + j) * 4 + e) * 256 + slot;
+            double v = __ldcg(first + off);
+            for (int c = 1; c < S; ++c) v += __ldcg(first + (size_t)c * 64 * 256 + off);
+            acc[i][j][e] = v;
+          }
+      if (lane == 0) p.arrivals[(u / S) * CONSUMERS + warp] = 0;
     }
 
     // Epilogue: accumulator e of block (i, j) is row g + 8 (e >> 1), column
@@ -217,7 +266,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 }  // namespace
 
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s) {
-  const long tiles = a.tile_list ? a.ntiles : (long)a.tiles_m * a.tiles_n;
+  const long tiles = (a.tile_list ? a.ntiles : (long)a.tiles_m * a.tiles_n) * a.splits;
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "dgemm: too many tiles");
   static bool configured = false;

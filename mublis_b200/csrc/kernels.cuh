@@ -4,6 +4,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 // Logical operand view for packing.  Element (r, c) of the stored operand
@@ -140,6 +142,24 @@ struct SimtGemmArgs {
   int m, n, k;
   T alpha, beta;
   int jp, ji, pi;
+  // Scheduling, filled by the launcher when the caller passes a SimtPolicy:
+  // persistent CTAs take units (tile, k-chunk) from a counter.  Left at
+  // these defaults, every CTA computes the one tile of its block index.
+  const int2 *tile_list = nullptr;  // (tm, tn) of the tiles to compute, or null: all tiles
+  int ntiles = 0;                   // tiles scheduled (0: all tiles, one per CTA)
+  int splits = 1;                   // k-chunks per tile (split-K)
+  int *work = nullptr;              // unit counter (zeroed): persistent CTAs
+  int *arrivals = nullptr;          // per tile: k-chunks finished (zeroed), splits > 1
+  T *partials = nullptr;            // per unit: its k-chunk's sums, splits > 1
+};
+
+// What the launcher needs to schedule a call on persistent CTAs with
+// split-K: the whole call's output size (a column panel of a larger call
+// carries the call's m and n, so every panel splits its tiles' k ranges as
+// the whole call would, and panels stay bit-identical to the one-call
+// result).
+struct SimtPolicy {
+  long m_full, n_full;
 };
 
 // Plain FP64 GEMM on the FP64 tensor pipe over PACK_FRAG64 panels.
@@ -157,6 +177,13 @@ struct DmmaGemmArgs {
   int *err;
   unsigned long long wait_ns;  // bound of every mbarrier wait
   int stall;                   // failure-detection test: the producer issues no loads
+  // Split-K: each tile's k range in `splits` chunks (units tile * splits +
+  // chunk, taken round-robin by the persistent CTAs); with splits > 1 every
+  // chunk stores its sums in `partials` and the last of a tile's chunks to
+  // finish (counted in `arrivals`, zeroed) adds them in chunk order.
+  int splits = 1;
+  int *arrivals = nullptr;
+  double *partials = nullptr;
 };
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s);
 constexpr int B200_DMMA_TILE = 128, B200_DMMA_BK = 16;
@@ -173,8 +200,33 @@ struct SimtConfig<double> {
   static constexpr int BM = 128, BN = 128, BK = 16;  // panel padding (tiles may be smaller)
 };
 
+// pol == nullptr: one tile per CTA, no scratch (the allocation-free entry
+// point); otherwise persistent CTAs with split-K and stream-ordered scratch.
 template <typename T>
-int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s);
+int launch_simt_gemm(const SimtGemmArgs<T> &a, cudaStream_t s, const SimtPolicy *pol = nullptr);
+
+// ---- output-tile scheduling shared by the persistent GEMM kernels (sched.cu)
+
+// The product's domain relations (mublis_l3_relation_t values).
+struct b200_tile_domain_t {
+  int jp, ji, pi;
+};
+
+// The BM x BN tiles of an m x n output that write under ji (the reference's
+// block_is_outside, l3_driver.c:145-147,165-171), heaviest first (stable),
+// as (tm, tn); costs, when given, receives each tile's k-blocks of BK after
+// clipping its k range to jp / pi (l3_driver.c:130,148-150,163,171).
+void b200_tile_list(long m, long n, long k, int BM, int BN, int BK, b200_tile_domain_t dom,
+                    std::vector<int2> *list, std::vector<int> *costs);
+
+// Split-K factor for a whole call (m_full x n_full x k) on `slots` resident
+// persistent CTAs that take units (tile, k-chunk) heaviest tile first: the
+// S in 1..16 (chunks of at least 8 k-blocks) whose simulated list schedule
+// ends first, counting a fixed start-up cost per unit; ties go to the
+// smaller S.  Depends only on its arguments (cached per shape), so every
+// column panel of a call splits its tiles as the whole call does.
+int b200_split_for(long m_full, long n_full, long k, int BM, int BN, int BK,
+                   b200_tile_domain_t dom, long slots);
 
 template <typename T>
 int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStream_t s);

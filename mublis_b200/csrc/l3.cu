@@ -138,6 +138,20 @@ int run_dmma(const b200_l3_desc_t *d) {
             cudaSuccess)
       st = b200_set_error(B200_ECUDA, "dgemm: tile list upload failed");
   }
+  // Split-K from the whole call's shape (column panels carry the call's m
+  // and n), so panels split their tiles' k ranges as the whole call does.
+  const int S = b200_split_for(d->policy_m > 0 ? d->policy_m : d->m,
+                               d->policy_n > 0 ? d->policy_n : d->n, ktot, B200_DMMA_TILE,
+                               B200_DMMA_TILE, B200_DMMA_BK, {dom.jp, dom.ji, dom.pi},
+                               b200_sm_count());
+  const long sched_tiles = list ? ntiles : (long)tiles_m * tiles_n;
+  void *split_ws = nullptr;
+  if (st == B200_OK && S > 1) {
+    const size_t ints = b200_round_up(sizeof(int) * sched_tiles * 8, 256);
+    st = b200_alloc(&split_ws, ints + sizeof(double) * (size_t)sched_tiles * S * 64 * 256);
+    if (st == B200_OK && cudaMemsetAsync(split_ws, 0, ints, s) != cudaSuccess)
+      st = b200_set_error(B200_ECUDA, "dgemm: split-K counters");
+  }
   if (st == B200_OK && (list == nullptr || ntiles > 0)) {
     DmmaGemmArgs g;
     g.ap = (const double *)ap;
@@ -165,8 +179,15 @@ int run_dmma(const b200_l3_desc_t *d) {
       g.wait_ns = limit;
       g.stall = 1;
     }
+    g.splits = S;
+    if (S > 1) {
+      g.arrivals = (int *)split_ws;
+      g.partials = (double *)((char *)split_ws +
+                              b200_round_up(sizeof(int) * sched_tiles * 8, 256));
+    }
     st = launch_dmma_gemm(g, s);
   }
+  b200_free(split_ws);
   b200_free(list);
   b200_free(ap);
   b200_free(bp);
@@ -206,7 +227,9 @@ int run_plain(const b200_l3_desc_t *d) {
     g.jp = d->product.domain.jp;
     g.ji = d->product.domain.ji;
     g.pi = d->product.domain.pi;
-    st = launch_simt_gemm<T>(g, s);
+    const SimtPolicy pol = {d->policy_m > 0 ? d->policy_m : d->m,
+                            d->policy_n > 0 ? d->policy_n : d->n};
+    st = launch_simt_gemm<T>(g, s, &pol);
   }
   b200_free(ap);
   b200_free(bp);

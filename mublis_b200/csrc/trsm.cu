@@ -25,6 +25,7 @@
 // alpha is applied once up front (the reference's alpha_eff on the first
 // block, trsm.c:96-97).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -43,6 +44,16 @@ constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
 // would cost more than it saves, so 1024 is used only from m >= 4096 and
 // n >= 2048.
 int leaf_order(long m, long n) { return m >= 4096 && n >= 2048 ? 1024 : 512; }
+
+// Solves use the fused leaf kernel (trsm_leaf.cu) unless
+// MUBLIS_B200_TRSM=inverse selects the inverted-diagonal-block products.
+bool fused_leaves() {
+  static const bool on = [] {
+    const char *e = getenv("MUBLIS_B200_TRSM");
+    return !(e && !strcmp(e, "inverse"));
+  }();
+  return on;
+}
 
 // One CTA per LEAF block: thread j computes column j of the inverse of the
 // block's (lower or upper) triangle by substitution, L x = e_j.  Rows past
@@ -203,11 +214,39 @@ int for_each_chain(const Chains &ch, Build build) {
   return B200_OK;
 }
 
+// Inverted diagonal blocks of one triangle (FP32: the leaves of the solve,
+// applied as products), or (FP64) the packed leaves of the fused
+// GEMMTRSM kernel (trsm_leaf.cu).
+struct TrsmPrep {
+  void *inv;
+  long big;
+  void *leaf;
+};
+
 template <typename T>
-int trsm_rec(const Chains &ch, const T *inv, const long big, long r0, long r1) {
+int trsm_rec(const Chains &ch, const TrsmPrep *prep, long r0, long r1) {
   const b200_trsm_desc_t &d0 = *ch.d[0];
   const bool lower = d0.uplo == MUBLIS_LOWER;
+  const T *inv = (const T *)prep->inv;
+  const long big = prep->big;
   long rows = r1 - r0;
+  if (rows <= big && prep->leaf) {
+    // Fused leaf: the diagonal blocks solved in shared memory, the updates
+    // between them on the tensor pipe, every right-hand side of the chain.
+    for (int c = 0; c < ch.count; ++c) {
+      const b200_trsm_desc_t &d = *ch.d[c];
+      T *b = (T *)d.b;
+      const T *pack = (const T *)prep->leaf + (r0 / big) * b200_trsm_leaf_stride();
+      static_assert(sizeof(T) == 4 || sizeof(T) == 8, "FP32 / FP64");
+      T *first = lower ? b + r0 * d.rs_b : b + (r1 - 1) * d.rs_b;
+      void *prev = b200_override_stream((void *)ch.streams[c]);
+      const int st = b200_trsm_leaf_solve(d.dtype, pack, (int)rows, first,
+                                          lower ? d.rs_b : -d.rs_b, d.cs_b, d.n);
+      b200_override_stream(prev);
+      B200_TRY(st);
+    }
+    return B200_OK;
+  }
   if (rows <= big) {
     // X_b = inv(A_bb) B_b in place: the packed path packs B_b before the
     // product writes it.  Plain precision: the diagonal-block solve is FP64
@@ -242,7 +281,7 @@ int trsm_rec(const Chains &ch, const T *inv, const long big, long r0, long r1) {
   // Rows solved first (src) and rows updated by them (dst).
   long s0 = lower ? r0 : mid, s1 = lower ? mid : r1;
   long t0 = lower ? mid : r0, t1 = lower ? r1 : mid;
-  B200_TRY(trsm_rec<T>(ch, inv, big, s0, s1));
+  B200_TRY(trsm_rec<T>(ch, prep, s0, s1));
   B200_TRY(for_each_chain(ch, [&](const b200_trsm_desc_t &d) {
     const T *a = (const T *)d.a;
     T *b = (T *)d.b;
@@ -264,17 +303,31 @@ int trsm_rec(const Chains &ch, const T *inv, const long big, long r0, long r1) {
     g.cs_c = d.cs_b;
     return g;
   }));
-  return trsm_rec<T>(ch, inv, big, t0, t1);
+  return trsm_rec<T>(ch, prep, t0, t1);
 }
 
-// Inverted diagonal blocks of one triangle (the leaves of the solve).
-struct TrsmPrep {
-  void *inv;
-  long big;
-};
+// Pack every leaf of op(A) for the fused kernel (reciprocal diagonal; FP64
+// panel blocks in MMA fragment order, FP32 column-major).
+int build_leaves(const b200_trsm_desc_t *d, TrsmPrep *p) {
+  const long leaves = b200_ceil_div(d->m, b200_trsm_leaf_rows());
+  const size_t elt = d->dtype == B200_F32 ? sizeof(float) : sizeof(double);
+  void *pack = nullptr;
+  B200_TRY(b200_alloc(&pack, elt * leaves * b200_trsm_leaf_stride()));
+  const int st = b200_trsm_leaf_pack(d->dtype, d->a, d->rs_a, d->cs_a, d->m,
+                                     d->uplo == MUBLIS_LOWER, d->unit_diag != 0, pack);
+  if (st != B200_OK) {
+    b200_free(pack);
+    return st;
+  }
+  p->inv = nullptr;
+  p->big = b200_trsm_leaf_rows();
+  p->leaf = pack;
+  return B200_OK;
+}
 
 template <typename T>
 int build_inverse(const b200_trsm_desc_t *d, TrsmPrep *p) {
+  if (fused_leaves()) return build_leaves(d, p);
   cudaStream_t s = b200_cur_stream();
   T *inv = nullptr, *tmp = nullptr;
   const long big = leaf_order(d->m, d->policy_n > 0 ? d->policy_n : d->n);
@@ -294,20 +347,19 @@ int build_inverse(const b200_trsm_desc_t *d, TrsmPrep *p) {
   }
   p->inv = inv;
   p->big = big;
+  p->leaf = nullptr;
   return B200_OK;
 }
 
 template <typename T>
 int trsm_solve(const b200_trsm_desc_t *d) {
   cudaStream_t s = b200_cur_stream();
-  TrsmPrep own = {nullptr, 0};
+  TrsmPrep own = {nullptr, 0, nullptr};
   const TrsmPrep *prep = (const TrsmPrep *)d->prep;
   if (!prep) {
     B200_TRY(build_inverse<T>(d, &own));
     prep = &own;
   }
-  const T *inv = (const T *)prep->inv;
-  const long big = prep->big;
   int st = B200_OK;
   if (st == B200_OK) {
     // The right-hand sides are independent: a large solve runs its two
@@ -329,7 +381,7 @@ int trsm_solve(const b200_trsm_desc_t *d) {
         st = b200_set_error(B200_ECUDA, "trsm: stream fork failed");
       if (st == B200_OK) {
         const Chains ch = {{&h0, &h1}, {s, s2}, 2};
-        st = trsm_rec<T>(ch, inv, big, 0, d->m);
+        st = trsm_rec<T>(ch, prep, 0, d->m);
       }
       // Join even after a failure, so nothing of the second chain is left
       // running on the scratch freed below.
@@ -340,10 +392,11 @@ int trsm_solve(const b200_trsm_desc_t *d) {
       if (e1) cudaEventDestroy(e1);
     } else {
       const Chains ch = {{d, nullptr}, {s, nullptr}, 1};
-      st = trsm_rec<T>(ch, inv, big, 0, d->m);
+      st = trsm_rec<T>(ch, prep, 0, d->m);
     }
   }
   b200_free(own.inv);
+  b200_free(own.leaf);
   return st;
 }
 
@@ -354,7 +407,7 @@ extern "C" int b200_trsm_prepare(const b200_trsm_desc_t *d, void **prep) {
   if (d->m <= 0) return B200_OK;
   if (d->uplo != MUBLIS_LOWER && d->uplo != MUBLIS_UPPER)
     return b200_set_error(B200_EINVAL, "trsm: uplo must be lower or upper");
-  TrsmPrep *p = new TrsmPrep{nullptr, 0};
+  TrsmPrep *p = new TrsmPrep{nullptr, 0, nullptr};
   const int st = d->dtype == B200_F32 ? build_inverse<float>(d, p) : build_inverse<double>(d, p);
   if (st != B200_OK) {
     delete p;
@@ -368,6 +421,7 @@ extern "C" void b200_trsm_release(void *prep) {
   TrsmPrep *p = (TrsmPrep *)prep;
   if (!p) return;
   b200_free(p->inv);  // stream-ordered after the panels on this stream
+  b200_free(p->leaf);
   delete p;
 }
 

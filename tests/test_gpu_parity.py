@@ -414,3 +414,25 @@ def test_trsm_large_solve_with_1024_leaves(lib, dtype, uplo):
     assert fn(0, uplo, 0, 0, n, n, 1.0, a.ctypes.data, 1, n, host.ctypes.data, 1, n) == 0, \
         mb.last_error(lib)
     np.testing.assert_array_equal(host, dev)
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+@pytest.mark.parametrize("m,n", [(16, 1), (17, 33), (511, 65), (513, 31), (1040, 100),
+                                 (1537, 257)])
+@pytest.mark.parametrize("flags", [dict(right=False, lower=True, ta=False, unit=False),
+                                   dict(right=False, lower=False, ta=False, unit=True),
+                                   dict(right=False, lower=True, ta=True, unit=False),
+                                   dict(right=True, lower=False, ta=False, unit=False)],
+                         ids=["LLN", "LUNu", "LLT", "RUN"])
+def test_trsm_leaf_boundaries(lib, dtype, m, n, flags):
+    """Solves whose order falls on and around the fused kernel's 16-row
+    diagonal blocks and 512-row leaves, with right-hand-side counts around
+    its 32-column CTAs, in both triangles, both layouts of op(A), unit and
+    non-unit diagonals, and from the right: against the oracle (relative
+    forward error <= 4 * order * u)."""
+    case = dict(routine="trsm", dtype=dtype, order="F", m=m, n=n, k=0, alpha=0.75, seed=17,
+                **flags)
+    a, b, c0, out = run_lib(lib, case)
+    ref = run_oracle(case)
+    assert np.isfinite(out).all()
+    assert cs.normwise_error(case, out, ref, a, b, c0) <= tol_of(case)
