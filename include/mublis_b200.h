@@ -42,6 +42,11 @@ void *mublis_b200_get_stream(void);
  *   both: "ozaki2" or "ozaki2:<moduli>" (int8 residues modulo up to 16
  *        moduli, exact int32 products, Chinese-remainder reconstruction;
  *        default 16 moduli for FP64, 8 for FP32)
+ *   both: "ozaki2@<target>" (e.g. "ozaki2@1e-16") -- the modular form with
+ *        the fewest moduli whose normwise error, measured on a calibration
+ *        block of the call (mublis_b200_ozaki2_autotune), is within the
+ *        target; the choice is cached per precision, power-of-two bucket of
+ *        k and target (and saved in the tuned table)
  *   both: "auto" -- per call, the fastest form whose error is no worse than
  *        plain: FP32 uses fp16x3 when min(m, n) >= 4096 and k >= 2048,
  *        bf16x6 when min(m, n) and k are >= 512, FP64 uses
@@ -55,6 +60,21 @@ int mublis_b200_set_form(char dtype, const char *form);
 unsigned long long mublis_b200_launch_count(void);
 int mublis_b200_profile_enable(int on);
 int mublis_b200_profile_read(char *buf, unsigned long len);
+
+/* Modulus-count autotuner of the modular Ozaki form.  For C = op(A) op(B)
+ * (device pointers; m x n x k; strides as in mublis_{s,d}gemm), computes a
+ * calibration block -- the leading min(m, 256) x min(n, 256) of the product
+ * over the whole k -- with a compensated (Dot2) dot product on the device,
+ * runs the form on it with 6 .. 16 moduli (FP32: 6 .. 8) from the fewest up
+ * and picks the first whose normwise error ||C_N - C_ref||_F /
+ * (||A_blk||_F ||B_blk||_F) is <= target_err (16 / 8 if none is).  The
+ * choice is recorded for later "ozaki2@<target_err>" calls of the same
+ * precision and power-of-two bucket of k.  *moduli gets the count,
+ * *measured_err (may be NULL) its measured error.  dtype 's' or 'd'. */
+int mublis_b200_ozaki2_autotune(char dtype, mublis_trans_t trans_a, mublis_trans_t trans_b, int m,
+                                int n, int k, const void *a, int rs_a, int cs_a, const void *b,
+                                int rs_b, int cs_b, double target_err, int *moduli,
+                                double *measured_err);
 
 /* Failure-detection test of the bounded device waits.  Arms a one-shot
  * stall for the next launch of the FP64 tensor-pipe GEMM kernel in the

@@ -119,6 +119,9 @@ EXTENSIONS = {
     "mublis_b200_profile_enable": ([_I], _I),
     "mublis_b200_profile_read": ([ctypes.c_char_p, ctypes.c_ulong], _I),
     "mublis_b200_test_stall_next": ([ctypes.c_ulonglong], _I),
+    "mublis_b200_ozaki2_autotune": ([ctypes.c_char, _I, _I, _I, _I, _I, _P, _I, _I, _P, _I, _I,
+                                     ctypes.c_double, ctypes.POINTER(_I),
+                                     ctypes.POINTER(ctypes.c_double)], _I),
     "mublis_b200_fill_s": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_b200_fill_d": ([_P, _L, _L, _L, _U32, _U32, _I], _I),
     "mublis_get_context": ([_P], _I),

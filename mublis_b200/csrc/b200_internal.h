@@ -41,9 +41,13 @@ enum { B200_FORM_AUTO = -1, B200_FORM_PLAIN = 0, B200_FORM_BF16X3 = 1, B200_FORM
        B200_FORM_OZAKI2 = 5, B200_FORM_FP16X3 = 6 /* FP32 via scaled fp16 hi/lo, 3 products */ };
 
 /* Parse a form name ("plain", "bf16x3", "bf16x6", "fp16x3", "ozaki[:s]",
- * "ozaki2[:N]", "auto"); B200_FORM_AUTO for anything else.  *slices gets s or N when
- * given (slices may be NULL). */
-int b200_parse_form(const char *s, int *slices);
+ * "ozaki2[:N]", "ozaki2@<target error>", "auto"); B200_FORM_AUTO for
+ * anything else.  *slices gets s or N, *target the error target, when given
+ * (either may be NULL). */
+int b200_parse_form(const char *s, int *slices, double *target);
+/* The "ozaki2@<target>" error target of a precision's default form (0:
+ * none). */
+double b200_get_default_target(int dtype);
 
 /* Loads the tuned-tile table named by MUBLIS_B200_TUNE_FILE, if any (called
  * once at initialisation). */

@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "../../include/mublis_b200.h"
+#include "tc_gemm.cuh"
 
 namespace {
 
@@ -469,6 +470,7 @@ int tune_save(const char *path) {
             text += line;
           }
   }
+  b200_ozaki2_table_lines(&text);
   const std::string tmp = std::string(path) + ".tmp";
   FILE *f = fopen(tmp.c_str(), "w");
   if (!f) return b200_set_error(B200_EINVAL, "tune: cannot write the table file");
@@ -492,6 +494,10 @@ int tune_load(const char *path, int *entries) {
     line[strcspn(line, "\r\n")] = 0;
     if (key == line) {
       while (fgets(line, sizeof line, f)) {
+        if (!strncmp(line, "ozaki2 ", 7)) {
+          if (b200_ozaki2_table_parse(line)) ++loaded;
+          continue;
+        }
         int dt, c, b, v;
         if (sscanf(line, "gemm %d %d %d %d", &dt, &c, &b, &v) != 4) continue;
         if (dt < 0 || dt > 1 || c < 0 || c >= NCLASS || b < 0 || b >= 32 || v < 0 ||
@@ -996,7 +1002,10 @@ extern "C" int mublis_b200_tune_load(const char *path, int *entries) {
   return tune_load(path, entries);
 }
 
+void b200_tune_save_env() { b200_tune_autosave(); }
+
 extern "C" int mublis_b200_tune_reset(void) {
+  b200_ozaki2_table_reset();
   std::lock_guard<std::mutex> lk(g_tune_mu);
   memset(g_tuned, 0, sizeof g_tuned);
   return B200_OK;

@@ -19,6 +19,29 @@ struct PackView {
   int mask_rel;
 };
 
+// Logical element (r, c) of a view (frame/l1m/packm.c:40-71): zero outside
+// the mask relation, the stored triangle reflected for a symmetric operand,
+// zero outside it for a triangular one (unit / inverted diagonal applied).
+// Elements outside the stored triangle are never read.
+template <typename T>
+__device__ __forceinline__ T load_logical(const PackView &v, long r, long c) {
+  const T *x = (const T *)v.x;
+  if (!b200_rel(v.mask_rel, c, r)) return T(0);
+  long delta = r - c;
+  bool stored = v.uplo == MUBLIS_LOWER ? delta >= 0 : (v.uplo == MUBLIS_UPPER ? delta <= 0 : true);
+  if (v.struc == MUBLIS_STRUC_SYMMETRIC) {
+    return stored ? x[r * v.rs + c * v.cs] : x[c * v.rs + r * v.cs];
+  }
+  if (v.struc == MUBLIS_STRUC_TRIANGULAR) {
+    if (!stored) return T(0);
+    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_UNIT) return T(1);
+    T val = x[r * v.rs + c * v.cs];
+    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_INVERT) val = T(1) / val;
+    return val;
+  }
+  return x[r * v.rs + c * v.cs];
+}
+
 // Output orientation of a packed panel.  The panel covers mn in [0, mn_pad)
 // and kk in [kk0, kk1); logical element (mn, kk - kk0) is taken from the
 // view, as (r, c) = (mn, kk) for an A-side view or (kk, mn) for a B-side

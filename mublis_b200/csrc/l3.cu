@@ -262,6 +262,13 @@ extern "C" int b200_l3_run(const b200_l3_desc_t *d) {
     if (d->form == B200_FORM_POLICY || (d->form == B200_FORM_AUTO &&
                                         b200_get_default_form(d->dtype) == B200_FORM_POLICY))
       e.slices = form == B200_FORM_OZAKI ? 8 : 0;  // 0: the form's default count
+    // "ozaki2@<target>": the modulus count measured for the target error
+    // (cached per precision, k bucket and target).
+    const double target = b200_get_default_target(d->dtype);
+    if (form == B200_FORM_OZAKI2 && d->form == B200_FORM_AUTO && target > 0 && d->slices == 0 &&
+        b200_get_default_form(d->dtype) == B200_FORM_OZAKI2 &&
+        b200_get_default_slices(d->dtype) == 0)
+      B200_TRY(b200_ozaki2_choice(&e, target, &e.slices, nullptr, 0));
     return tc_run_ozaki(&e);
   }
   if (d->dtype == B200_F32) return run_plain<float>(d);

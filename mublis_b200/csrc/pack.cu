@@ -21,25 +21,6 @@
 namespace {
 
 template <typename T>
-__device__ __forceinline__ T load_logical(const PackView &v, long r, long c) {
-  const T *x = (const T *)v.x;
-  if (!b200_rel(v.mask_rel, c, r)) return T(0);
-  long delta = r - c;
-  bool stored = v.uplo == MUBLIS_LOWER ? delta >= 0 : (v.uplo == MUBLIS_UPPER ? delta <= 0 : true);
-  if (v.struc == MUBLIS_STRUC_SYMMETRIC) {
-    return stored ? x[r * v.rs + c * v.cs] : x[c * v.rs + r * v.cs];
-  }
-  if (v.struc == MUBLIS_STRUC_TRIANGULAR) {
-    if (!stored) return T(0);
-    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_UNIT) return T(1);
-    T val = x[r * v.rs + c * v.cs];
-    if (delta == 0 && v.diag == MUBLIS_PACKM_DIAG_INVERT) val = T(1) / val;
-    return val;
-  }
-  return x[r * v.rs + c * v.cs];
-}
-
-template <typename T>
 __global__ void __launch_bounds__(256) pack_kernel(PackView v, bool b_side, long mn_len,
                                                    long k_len, long kk0, long kk1, PackOut o,
                                                    bool mn_fast_load) {

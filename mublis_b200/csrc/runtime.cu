@@ -28,6 +28,7 @@ std::atomic<unsigned long long> g_launches{0};
 
 int g_default_form[2] = {B200_FORM_PLAIN, B200_FORM_PLAIN};
 int g_default_slices[2] = {0, 0};  // per dtype: slice / modulus count, 0 = form default
+double g_default_target[2] = {0.0, 0.0};  // per dtype: "ozaki2@<target>" error target, 0 = none
 
 thread_local cudaStream_t t_stream = nullptr;
 thread_local bool t_stream_owned = false;
@@ -66,8 +67,9 @@ void do_init() {
   }
   int slices = 0;
   int sslices = 0;
-  int sf = b200_parse_form(getenv("MUBLIS_B200_SFORM"), &sslices);
-  int df = b200_parse_form(getenv("MUBLIS_B200_DFORM"), &slices);
+  double starget = 0.0, dtarget = 0.0;
+  int sf = b200_parse_form(getenv("MUBLIS_B200_SFORM"), &sslices, &starget);
+  int df = b200_parse_form(getenv("MUBLIS_B200_DFORM"), &slices, &dtarget);
   if (sf == B200_FORM_PLAIN || sf == B200_FORM_BF16X3 || sf == B200_FORM_BF16X6 ||
       sf == B200_FORM_FP16X3 || sf == B200_FORM_OZAKI2 || sf == B200_FORM_POLICY)
     g_default_form[B200_F32] = sf;
@@ -76,6 +78,8 @@ void do_init() {
     g_default_form[B200_F64] = df;
   if (slices > 0) g_default_slices[B200_F64] = slices;
   if (sslices > 0) g_default_slices[B200_F32] = sslices;
+  if (df == B200_FORM_OZAKI2) g_default_target[B200_F64] = dtarget;
+  if (sf == B200_FORM_OZAKI2) g_default_target[B200_F32] = starget;
   g_init_status = B200_OK;
   b200_tune_autoload();
   // The allocation-free SGEMM's fixed scratch array is claimed here, at
@@ -234,7 +238,7 @@ int b200_sm_count(void) {
   return sms;
 }
 
-int b200_parse_form(const char *s, int *slices) {
+int b200_parse_form(const char *s, int *slices, double *target) {
   if (!s || !*s) return B200_FORM_AUTO;
   if (!strcmp(s, "plain")) return B200_FORM_PLAIN;
   if (!strcmp(s, "bf16x3")) return B200_FORM_BF16X3;
@@ -246,6 +250,11 @@ int b200_parse_form(const char *s, int *slices) {
     const char *tail = s + (mod ? 6 : 5);
     if (*tail == ':') {
       if (slices) *slices = atoi(tail + 1);
+    } else if (mod && *tail == '@') {
+      char *end = nullptr;
+      const double t = strtod(tail + 1, &end);
+      if (!(t > 0) || end == tail + 1 || *end) return B200_FORM_AUTO;
+      if (target) *target = t;
     } else if (*tail) {
       return B200_FORM_AUTO;
     }
@@ -255,6 +264,7 @@ int b200_parse_form(const char *s, int *slices) {
 }
 
 int b200_get_default_form(int dtype) { return g_default_form[dtype == B200_F64]; }
+double b200_get_default_target(int dtype) { return g_default_target[dtype == B200_F64]; }
 int b200_get_default_slices(int dtype) { return g_default_slices[dtype == B200_F64]; }
 
 int b200_set_default_form(int dtype, int form, int slices) {
@@ -266,8 +276,10 @@ int b200_set_default_form(int dtype, int form, int slices) {
       form != B200_FORM_OZAKI2 && form != B200_FORM_POLICY)
     return B200_EINVAL;
   g_default_form[dtype == B200_F64] = form;
-  // The count belongs to the form just set (0: that form's own default).
+  // The count and target belong to the form just set (0: that form's own
+  // default).
   g_default_slices[dtype == B200_F64] = slices > 0 ? slices : 0;
+  g_default_target[dtype == B200_F64] = 0.0;
   return B200_OK;
 }
 
@@ -591,9 +603,13 @@ void *mublis_b200_get_stream(void) {
 int mublis_b200_set_form(char dtype, const char *form) {
   B200_TRY(b200_init());
   int slices = 0;
-  int f = b200_parse_form(form, &slices);
+  double target = 0.0;
+  int f = b200_parse_form(form, &slices, &target);
   if (f == B200_FORM_AUTO) return B200_EINVAL;
-  return b200_set_default_form(dtype == 'd' ? B200_F64 : B200_F32, f, slices);
+  const int dt = dtype == 'd' ? B200_F64 : B200_F32;
+  B200_TRY(b200_set_default_form(dt, f, slices));
+  if (f == B200_FORM_OZAKI2) g_default_target[dt == B200_F64] = target;
+  return B200_OK;
 }
 
 unsigned long long mublis_b200_launch_count(void) { return g_launches.load(); }

@@ -300,7 +300,7 @@ extern "C" int b200_serve_l3(const b200_l3_desc_t *d) {
   r.small = b200_l3_is_plain_gemm(d) && mx <= S->cfg.small_max_dim;
   if (!r.small && r.l3.form == B200_FORM_AUTO) {
     int slices = 0;
-    int f = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
+    int f = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices, nullptr);
     r.l3.form = f;
     if (slices) r.l3.slices = slices;
   }
@@ -319,7 +319,7 @@ extern "C" int b200_serve_trsm(const b200_trsm_desc_t *d) {
   r.small = d->m <= 256 && d->alpha != 0.0;
   if (!r.small && r.tr.form == B200_FORM_AUTO) {
     int slices = 0;
-    r.tr.form = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices);
+    r.tr.form = b200_parse_form(d->dtype == B200_F64 ? S->cfg.dform : S->cfg.sform, &slices, nullptr);
     if (slices) r.tr.slices = slices;
   }
   r.scratch = r.small ? 0 : scratch_estimate(r);

@@ -6,3 +6,18 @@
 
 int tc_run_bf16(const b200_l3_desc_t *d, int form);
 int tc_run_ozaki(const b200_l3_desc_t *d);
+
+#include <string>
+
+// ozaki_tune.cu: the modulus count of the modular form for a target
+// normwise error, measured on a calibration block of the call (cached per
+// precision, k bucket and target; force = 1 measures again).
+int b200_ozaki2_choice(const b200_l3_desc_t *d, double target, int *moduli, double *measured,
+                       int force);
+// Tuned-table persistence of those choices (lines appended / parsed by the
+// table's save and load; reset clears them).
+void b200_ozaki2_table_lines(std::string *text);
+bool b200_ozaki2_table_parse(const char *line);
+void b200_ozaki2_table_reset();
+// grouped.cu: rewrites the table named by MUBLIS_B200_TUNE_FILE, if any.
+void b200_tune_save_env();

@@ -308,3 +308,61 @@ def test_dtrsm_8192_forms(lib):
         print(f"  dtrsm {form:8s} {nw:.3e}  {mx:.3e}")
     assert errs["plain"][0] <= 4 * n * 2.0 ** -53
     assert errs["ozaki2"][0] <= 4 * n * 2.0 ** -53
+
+
+@pytest.mark.parametrize("kind", [orc.UNIFORM, orc.WIDE], ids=["uniform", "wide"])
+def test_ozaki2_autotune_picks_fewest_moduli_for_target(lib, kind):
+    """mublis_b200_ozaki2_autotune (config 3b: the modulus count chosen for a
+    stated error): a looser target never takes more moduli than a tighter
+    one, the measured calibration error of the choice meets the target
+    (unless all 16 moduli were needed), and a call with form
+    "ozaki2@<target>" then meets the target on the whole product, against
+    double-double values of 512 sampled entries (within 2x: the choice was
+    measured on the leading 256 x 256 block)."""
+    torch = pytest.importorskip("torch")
+    n = 2048
+    a = orc.fill(n, n, np.float64, 14, 0, kind)
+    b = orc.fill(n, n, np.float64, 14, 1, kind)
+    ad = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    bd = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    rng = np.random.default_rng(6)
+    rows, cols = rng.integers(0, n, 512), rng.integers(0, n, 512)
+    hi, lo = orc.dd_gemm_entries(a, b, rows, cols)
+    den = np.linalg.norm(a) * np.linalg.norm(b)
+    chosen = []
+    for target in (1e-13, 1e-15, 1e-17):
+        nm, err = ctypes.c_int(), ctypes.c_double()
+        assert lib.mublis_b200_ozaki2_autotune(b"d", 0, 0, n, n, n, ad.data_ptr(), 1, n,
+                                               bd.data_ptr(), 1, n, target, ctypes.byref(nm),
+                                               ctypes.byref(err)) == 0, mb.last_error(lib)
+        assert 6 <= nm.value <= 16
+        assert err.value <= target or nm.value == 16, (target, nm.value, err.value)
+        chosen.append(nm.value)
+        assert lib.mublis_b200_set_form(b"d", f"ozaki2@{target!r}".encode()) == 0
+        c = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+        assert lib.mublis_dgemm(0, 0, n, n, n, 1.0, ad.data_ptr(), 1, n, bd.data_ptr(), 1, n,
+                                0.0, c.data_ptr(), 1, n) == 0, mb.last_error(lib)
+        lib.mublis_b200_set_form(b"d", b"plain")
+        d = c.cpu().numpy().T[rows, cols] - (hi + lo)
+        whole = np.sqrt((d ** 2).sum() * n * n / len(rows)) / den
+        if nm.value < 16:
+            assert whole <= 2 * target, (target, nm.value, whole)
+    print(f"\nozaki2 autotune, n=2048, draw={'wide' if kind else 'uniform'}: "
+          f"targets 1e-13/1e-15/1e-17 -> {chosen} moduli")
+    assert chosen == sorted(chosen)
+
+
+def test_ozaki2_autotune_fp32(lib):
+    """FP32 inputs: a target at plain FP32's level is met with at most the
+    default 8 moduli."""
+    torch = pytest.importorskip("torch")
+    n = 1024
+    a = torch.empty(n, n, dtype=torch.float32, device="cuda")
+    b = torch.empty(n, n, dtype=torch.float32, device="cuda")
+    lib.mublis_b200_fill_s(ctypes.c_void_p(a.data_ptr()), n, n, n, 15, 0, 0)
+    lib.mublis_b200_fill_s(ctypes.c_void_p(b.data_ptr()), n, n, n, 15, 1, 0)
+    nm, err = ctypes.c_int(), ctypes.c_double()
+    assert lib.mublis_b200_ozaki2_autotune(b"s", 0, 0, n, n, n, a.data_ptr(), 1, n, b.data_ptr(),
+                                           1, n, 1e-7, ctypes.byref(nm),
+                                           ctypes.byref(err)) == 0, mb.last_error(lib)
+    assert 6 <= nm.value <= 8 and err.value <= 1e-7, (nm.value, err.value)
