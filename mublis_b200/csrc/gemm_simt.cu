@@ -20,6 +20,7 @@
 // the reference's "no update" pass (:88-121).
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 #include <type_traits>
 #include <vector>
 
@@ -47,8 +48,10 @@ __device__ __forceinline__ void lds16(double (&d)[2], const double *p) {
   d[0] = v.x; d[1] = v.y;
 }
 
+// SPLIT: the split-K epilogue is compiled in (launched only when splits > 1,
+// so the unsplit kernel keeps its registers for the main loop).
 template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB,
-          bool PAIR = false>
+          bool PAIR = false, bool SPLIT = false>
 __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p) {
   constexpr int NT = 256;
   constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;
@@ -69,7 +72,7 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
   __shared__ int s_unit, s_last;
 
   const int tiles_m = (p.m + BM - 1) / BM, tiles_n = (p.n + BN - 1) / BN;
-  const int S = p.splits;
+  const int S = SPLIT ? p.splits : 1;
   const int ntiles = p.ntiles > 0 ? p.ntiles : tiles_m * tiles_n;
   const int units = ntiles * S;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p)
       // chunk of the tile to finish adds all S of them in chunk order --
       // the same order whichever CTA comes last -- and runs the epilogue.
       bool epilogue = true;
-      if (S > 1) {
+      if (SPLIT && S > 1) {
         constexpr int E = TM * TN;
         T *mine = p.partials + (size_t)u * E * NT;
 #pragma unroll
@@ -312,17 +315,25 @@ template <typename T, int BM, int BN, int WM, int WN, int ST, int MINB, bool PAI
 int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol) {
   constexpr int BK = SimtConfig<T>::BK;
   constexpr int E = (BM / WM / 4) * (BN / WN / 8);  // accumulators per thread
-  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR>;
+  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR, false>;
+  auto kern_split = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR, true>;
   const size_t smem = (size_t)ST * BK * (BM + BN) * sizeof(T);
   static int per_sm = 0;
   if (!per_sm) {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    per_sm = resident_per_sm(kern, smem);
+    B200_CUDA_TRY(
+        cudaFuncSetAttribute(kern_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    per_sm = std::min(resident_per_sm(kern, smem), resident_per_sm(kern_split, smem));
   }
   const long tiles = b200_ceil_div(a0.m, BM) * b200_ceil_div(a0.n, BN);
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL / 16) return b200_set_error(B200_EINVAL, "gemm: too many tiles");
-  if (!pol) {  // one tile per CTA, nothing allocated
+  // MUBLIS_B200_SIMT_PERSIST=0 keeps one tile per CTA for every call (tuning).
+  static const bool persist = [] {
+    const char *e = getenv("MUBLIS_B200_SIMT_PERSIST");
+    return !(e && !strcmp(e, "0"));
+  }();
+  if (!pol || !persist) {  // one tile per CTA, nothing allocated
     B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
     kern<<<(unsigned)tiles, 256, smem, s>>>(a0);
     B200_LAUNCH_CHECK();
@@ -342,7 +353,8 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
     ntiles = (long)list.size();
     if (ntiles == 0) return B200_OK;
   }
-  const int S = b200_split_for(pol->m_full, pol->n_full, a.k, BM, BN, BK, dom, slots);
+  // A split unit's 64 KB of partial sums cost about 4 k-block times.
+  const int S = b200_split_for(pol->m_full, pol->n_full, a.k, BM, BN, BK, dom, slots, 4.0);
   const long units = ntiles * S;
   const size_t ints = sizeof(int) * (size_t)(1 + ntiles);
   const size_t list_bytes = sizeof(int2) * list.size();
@@ -364,7 +376,8 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
     a.splits = S;
     a.partials = S > 1 ? (T *)(scratch + off_part) : nullptr;
     B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
-    kern<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
+    if (S > 1) kern_split<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
+    else kern<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
     if (cudaGetLastError() != cudaSuccess) st = b200_set_error(B200_ECUDA, "gemm: launch failed");
   }
   b200_free(scratch);

@@ -245,11 +245,12 @@ void b200_tile_list(long m, long n, long k, int BM, int BN, int BK, b200_tile_do
 // Split-K factor for a whole call (m_full x n_full x k) on `slots` resident
 // persistent CTAs that take units (tile, k-chunk) heaviest tile first: the
 // S in 1..16 (chunks of at least 8 k-blocks) whose simulated list schedule
-// ends first, counting a fixed start-up cost per unit; ties go to the
-// smaller S.  Depends only on its arguments (cached per shape), so every
+// ends first, counting a fixed start-up cost per unit and split_cost
+// (k-block times) more per split unit; S > 1 is taken only when it beats
+// S = 1 by 10%.  Depends only on its arguments (cached per shape), so every
 // column panel of a call splits its tiles as the whole call does.
 int b200_split_for(long m_full, long n_full, long k, int BM, int BN, int BK,
-                   b200_tile_domain_t dom, long slots);
+                   b200_tile_domain_t dom, long slots, double split_cost);
 
 template <typename T>
 int launch_scale(int m, int n, T beta, T *c, long rs, long cs, int ji, cudaStream_t s);

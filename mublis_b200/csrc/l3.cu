@@ -143,7 +143,7 @@ int run_dmma(const b200_l3_desc_t *d) {
   const int S = b200_split_for(d->policy_m > 0 ? d->policy_m : d->m,
                                d->policy_n > 0 ? d->policy_n : d->n, ktot, B200_DMMA_TILE,
                                B200_DMMA_TILE, B200_DMMA_BK, {dom.jp, dom.ji, dom.pi},
-                               b200_sm_count());
+                               b200_sm_count(), 8.0);  // 128 KB of partials per split unit
   const long sched_tiles = list ? ntiles : (long)tiles_m * tiles_n;
   void *split_ws = nullptr;
   if (st == B200_OK && S > 1) {

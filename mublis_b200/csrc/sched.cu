@@ -15,6 +15,7 @@
 // has few tiles and a long k (SYRK with n = 1024, k = 8192: 36 tiles), keeps
 // every SM busy.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <queue>
@@ -57,10 +58,16 @@ void b200_tile_list(long m, long n, long k, int BM, int BN, int BK, b200_tile_do
 namespace {
 
 // Per-unit cost beyond its k-blocks, in k-block times: fetching the unit,
-// filling the copy pipeline and the epilogue (measured on the FP32 kernel:
-// a 128 x 128 tile's k-block takes ~2 us, a unit's start-up ~3 us); a split
-// tile adds the store and reload of its partial sums.
-constexpr double UNIT_COST = 1.5, SPLIT_COST = 0.5;
+// filling the copy pipeline and the epilogue.  A split unit also stores its
+// partial sums and the tile's last one reloads them all, and concurrent
+// k-chunks of one tile share less of the operand panels in L2; the
+// caller's split_cost covers that.  Measured on B200: a split that the
+// simulation credits with under 10% is slower in practice (SGEMM 4096^3
+// on 296 CTAs: S = 2 modelled 9% faster, measured 4.5% slower), while
+// tile-starved calls gain severalfold (SYRK n = 1024, k = 8192: 36 tiles,
+// FP32 10.9 -> 27.8 TF/s, FP64 7.2 -> 19.9), so S > 1 must beat S = 1 by
+// 10% in the model.
+constexpr double UNIT_COST = 1.5, SPLIT_GAIN = 0.9;
 constexpr int MAX_SPLITS = 16, MIN_CHUNK = 8;
 constexpr long MAX_SIM_UNITS = 1 << 16;
 
@@ -85,14 +92,21 @@ double simulate(const std::vector<double> &units, long slots) {
 }
 
 std::mutex g_mu;
-std::map<std::tuple<long, long, long, int, int, int, int, int, int, long>, int> g_cache;
+std::map<std::tuple<long, long, long, int, int, int, int, int, int, long, double>, int> g_cache;
 
 }  // namespace
 
 int b200_split_for(long m_full, long n_full, long k, int BM, int BN, int BK,
-                   b200_tile_domain_t dom, long slots) {
+                   b200_tile_domain_t dom, long slots, double split_cost) {
   if (m_full <= 0 || n_full <= 0 || k <= 0 || slots <= 0) return 1;
-  const auto key = std::make_tuple(m_full, n_full, k, BM, BN, BK, dom.jp, dom.ji, dom.pi, slots);
+  // MUBLIS_B200_SPLIT=<S> fixes the split count (1: no split-K), for tuning.
+  static const int forced = [] {
+    const char *e = getenv("MUBLIS_B200_SPLIT");
+    return e ? atoi(e) : 0;
+  }();
+  if (forced > 0) return std::min(forced, MAX_SPLITS);
+  const auto key = std::make_tuple(m_full, n_full, k, BM, BN, BK, dom.jp, dom.ji, dom.pi, slots,
+                                   split_cost);
   {
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(key);
@@ -104,7 +118,7 @@ int b200_split_for(long m_full, long n_full, long k, int BM, int BN, int BK,
   int smax = std::min(MAX_SPLITS, std::max(1, heaviest / MIN_CHUNK));
   while (smax > 1 && (long)costs.size() * smax > MAX_SIM_UNITS) --smax;
   int best = 1;
-  double best_t = 0;
+  double best_t = 0, t1 = 0;
   std::vector<double> units;
   for (int S = 1; S <= smax; ++S) {
     units.clear();
@@ -112,11 +126,14 @@ int b200_split_for(long m_full, long n_full, long k, int BM, int BN, int BK,
       const int per = (c + S - 1) / S;
       for (int q = 0; q < S; ++q) {
         const int len = std::max(0, std::min(per, c - q * per));
-        units.push_back(len + UNIT_COST + (S > 1 ? SPLIT_COST : 0.0));
+        units.push_back(len + UNIT_COST + (S > 1 ? split_cost : 0.0));
       }
     }
     const double t = simulate(units, slots);
-    if (S == 1 || t < 0.99 * best_t) {
+    if (S == 1) {
+      t1 = t;
+      best_t = t;
+    } else if (t < SPLIT_GAIN * t1 && t < best_t) {  // a split must win by 10%
       best = S;
       best_t = t;
     }

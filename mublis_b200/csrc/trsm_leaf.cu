@@ -13,15 +13,18 @@
 // cyclically so that every warp keeps working as the solve moves down).  For
 // each diagonal block d of 16 rows:
 //   * the warp that owns block d + 1 first applies block d's update to it,
-//     then solves it against the reciprocal diagonal (one lane per column,
-//     FP64, in shared memory) and writes it out -- so the next block is
-//     ready by the time the other warps finish their updates (look-ahead);
+//     then solves it in shared memory, X = inv(D) R with the inverse of its
+//     16 x 16 diagonal block -- so the next block is ready by the time the
+//     other warps finish their updates (look-ahead);
 //   * every other warp applies X_d to its blocks below: B_rb -= A_rb,d X_d,
-//     16 x 32 x 16 per block as m16n8k4 .f64 MMAs on the tensor pipe.
+//     16 x 32 x 16 per block as m16n8k4 .f64 MMAs on the tensor pipe;
+//   * all threads write X_d to B (off the owner's critical path).
 // One barrier per block.  The leaf's A is packed once per solve
 // (trsm_leaf_pack_kernel) into one contiguous segment per step -- the
 // column of 16 x 16 blocks below the diagonal block in MMA fragment order,
-// then the next diagonal block with its reciprocal diagonal -- and one
+// then the inverse of the next diagonal block, formed by substitution
+// against the reciprocal diagonal (the reference's inverted-diagonal
+// packing, packm.c:143-144, carried to the whole 16 x 16 block) -- and one
 // thread streams segments into a 3-deep shared-memory ring with 1-D bulk
 // copies (TMA), two steps ahead.  Every wait is bounded (tc_common.cuh); a
 // CTA that gives up waits for its own copies and returns, and the call
@@ -87,8 +90,9 @@ __device__ T leaf_elem(const LeafPackArgs &a, long r0, int rows, int i, int p) {
 
 // grid (LEAF_BLOCKS, leaves * LEAF_BLOCKS), 256 threads: blockIdx.y =
 // leaf * LEAF_BLOCKS + s; s = 0 is diagonal block 0, s = d + 1 is step d's
-// segment, whose block x is panel block d + 1 + x (FP64: MMA fragment order;
-// FP32: column-major) or, for the last x, diagonal block d + 1 (row-major).
+// segment, whose block x is panel block d + 1 + x or, for the last x, the
+// inverse of diagonal block d + 1.  FP64 blocks are stored in MMA
+// A-fragment order; FP32 panel blocks column-major, inverses row-major.
 template <typename T>
 __global__ void __launch_bounds__(256) trsm_leaf_pack_kernel(const LeafPackArgs a) {
   __shared__ T tile[LB][LB + 1];
@@ -118,9 +122,30 @@ __global__ void __launch_bounds__(256) trsm_leaf_pack_kernel(const LeafPackArgs 
   const int ri = rows_fast ? tid % LB : tid / LB, pi = rows_fast ? tid / LB : tid % LB;
   tile[ri][pi] = leaf_elem<T>(a, r0, rows, bi * LB + ri, bp * LB + pi);
   __syncthreads();
-  T *out = (T *)a.out + (long)leaf * a.leaf_stride + off;
   if (diag) {
-    out[tid] = tile[tid / LB][tid % LB];
+    // The block's inverse, column j by thread j: forward substitution
+    // L x = e_j against the reciprocal diagonal (tile[i][i] = 1 / a_ii, as
+    // the reference packs it, packm.c:143-144).
+    T x[LB];
+    if (tid < LB) {
+#pragma unroll
+      for (int i = 0; i < LB; ++i) {
+        T r = i == tid ? T(1) : T(0);
+#pragma unroll
+        for (int q = 0; q < i; ++q) r = fma(-tile[i][q], x[q], r);
+        x[i] = r * tile[i][i];
+      }
+    }
+    __syncthreads();
+    if (tid < LB) {
+#pragma unroll
+      for (int i = 0; i < LB; ++i) tile[i][tid] = x[i];
+    }
+    __syncthreads();
+  }
+  T *out = (T *)a.out + (long)leaf * a.leaf_stride + off;
+  if (diag && sizeof(T) == 4) {
+    out[tid] = tile[tid / LB][tid % LB];  // row-major
   } else if (sizeof(T) == 8) {
     // MMA A-fragment order: (ks * 32 + lane) * 2 + h holds row g + 8h,
     // column 4 ks + t (lane = 4 g + t).
@@ -153,7 +178,8 @@ constexpr size_t leaf_smem() {
 // column 2 t + (e & 1)); panel blocks are packed in A-fragment order.
 // FP32: the updates are packed FP32 FMAs (two rows per instruction), one
 // lane per column, acc[q][i2] rows 2 i2 and 2 i2 + 1 of row block
-// warp + 8 q; panel blocks are packed column-major.
+// warp + 8 q; panel blocks are packed column-major, the diagonal blocks'
+// inverses row-major.
 template <typename T>
 __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_constant__ LeafArgs<T> p) {
   constexpr bool F64 = sizeof(T) == 8;
@@ -235,44 +261,79 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
   tc::fence_proxy_async();
   __syncthreads();
 
-  // Owner of block `blk` (warp blk % 8, accumulators acc[q] with q = blk / 8):
-  // its accumulators -> xout, solved by substitution against the diagonal
-  // block (row-major, reciprocal diagonal), one lane per column; the
-  // solution goes to xout and (coalesced) to B.
-  auto solve = [&](int q, int blk, const T *dg, T *xout) {
-    T x[LB];
+  // Owner of a block (warp blk % 8, accumulators acc[q] with q = blk / 8,
+  // fully updated): X = inv(D) R with the packed inverse of its diagonal
+  // block, into xout (row-major, XS_LD) for the other warps' updates.
+  auto solve = [&](int q, const T *dinv, T *xout) {
     if constexpr (F64) {
+      // R (accumulator layout) -> xout -> B fragments; X = inv(D) R as
+      // 4 x 4 m16n8k4 MMAs (A = inv(D) in fragment order), accumulated in
+      // the now free acc[q]; X -> xout.
 #pragma unroll
       for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
           xout[(g + 8 * (e >> 1)) * XS_LD + 8 * j + 2 * t + (e & 1)] = acc[q][j][e];
       __syncwarp();
+      double r[4][4];
 #pragma unroll
-      for (int i = 0; i < LB; ++i) x[i] = xout[i * XS_LD + lane];
+      for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) r[ks][j] = xout[(4 * ks + t) * XS_LD + 8 * j + g];
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[q][j][e] = 0.0;
+      const double2 *af = (const double2 *)dinv;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const double2 a = af[ks * 32 + lane];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[q][j], a.x, a.y, r[ks][j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          xout[(g + 8 * (e >> 1)) * XS_LD + 8 * j + 2 * t + (e & 1)] = acc[q][j][e];
     } else {
+      // One lane per column: x_i = sum_{p <= i} inv(D)_ip r_p (16 independent
+      // dot products over broadcast rows of the row-major inverse).
+      float r[LB];
 #pragma unroll
       for (int i2 = 0; i2 < 8; ++i2) {
-        x[2 * i2] = acc[q][i2].x;
-        x[2 * i2 + 1] = acc[q][i2].y;
+        r[2 * i2] = acc[q][i2].x;
+        r[2 * i2 + 1] = acc[q][i2].y;
+      }
+#pragma unroll
+      for (int i = 0; i < LB; ++i) {
+        const float4 *row = (const float4 *)(dinv + i * LB);
+        float x = 0.f;
+#pragma unroll
+        for (int v = 0; v <= i / 4; ++v) {
+          const float4 w = row[v];
+          x = fmaf(w.x, r[4 * v], x);
+          if (4 * v + 1 <= i) x = fmaf(w.y, r[4 * v + 1], x);
+          if (4 * v + 2 <= i) x = fmaf(w.z, r[4 * v + 2], x);
+          if (4 * v + 3 <= i) x = fmaf(w.w, r[4 * v + 3], x);
+        }
+        xout[i * XS_LD + lane] = x;
       }
     }
-#pragma unroll
-    for (int i = 0; i < LB; ++i) {
-      x[i] *= dg[i * LB + i];
-#pragma unroll
-      for (int r = i + 1; r < LB; ++r) x[r] = fma(-dg[r * LB + i], x[i], x[r]);
-    }
-#pragma unroll
-    for (int i = 0; i < LB; ++i) xout[i * XS_LD + lane] = x[i];
     __syncwarp();
+  };
+
+  // Solved block blk (in xsrc) -> B, by all 256 threads, coalesced along the
+  // stored matrix's unit stride.
+  auto write_block = [&](int blk, const T *xsrc) {
 #pragma unroll
-    for (int e = 0; e < LB; ++e) {
-      int r, c;
-      rc_of(e, r, c);
+    for (int h = 0; h < 2; ++h) {
+      const int idx = tid + h * THREADS;
+      const int r = rows_fast ? idx % LB : idx / NBC, c = rows_fast ? idx / LB : idx % NBC;
       const int row = blk * LB + r;
       const long col = col0 + c;
-      if (row < p.rows && col < p.n) p.b[row * p.rs_b + col * p.cs_b] = xout[r * XS_LD + c];
+      if (row < p.rows && col < p.n) p.b[row * p.rs_b + col * p.cs_b] = xsrc[r * XS_LD + c];
     }
   };
 
@@ -306,7 +367,7 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
   int d = 0;
   bool ok = tc::mbar_wait(&bar[RING], 0, abort_flag, p.err, p.wait_ns);
   if (__syncthreads_and(ok)) {
-    if (warp == 0) solve(0, 0, diag0, xs);
+    if (warp == 0) solve(0, diag0, xs);
     for (; d + 1 < nb; ++d) {
       ok = tc::mbar_wait(&bar[d % RING], (d / RING) & 1, abort_flag, p.err, p.wait_ns);
       // X_d is in xs[d & 1], segment d has landed, and every warp is done
@@ -316,20 +377,26 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
       const T *sg = seg + (d % RING) * SEG_MAX;
       const T *xd = xs + (d & 1) * LB * XS_LD;
       // (q runs over compile-time values so the accumulators stay in
-      // registers.)
+      // registers.)  The owner of block d + 1 goes first: its update and
+      // solve are the step's critical path.
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int rb = warp + 8 * q;
         if (rb == d + 1) {
           update(q, sg, xd);
-          solve(q, d + 1, sg + (nb - 1 - d) * BLK, xs + ((d + 1) & 1) * LB * XS_LD);
+          solve(q, sg + (nb - 1 - d) * BLK, xs + ((d + 1) & 1) * LB * XS_LD);
         }
       }
+      write_block(d, xd);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int rb = warp + 8 * q;
         if (rb > d + 1 && rb < nb) update(q, sg + (rb - d - 1) * BLK, xd);
       }
+    }
+    if (d + 1 == nb) {
+      __syncthreads();  // the last block, solved in the last step
+      write_block(d, xs + (d & 1) * LB * XS_LD);
     }
   } else {
     d = -1;  // diagonal block 0 never arrived
