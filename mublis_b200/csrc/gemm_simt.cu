@@ -18,6 +18,13 @@
 // Epilogue: C = alpha*acc + beta*C, and beta == 0 never reads C
 // (:111-112, :224-225).  A tile with an empty k-range writes beta*C, which is
 // the reference's "no update" pass (:88-121).
+//
+// Split-K (the reference's pc loop, l3_driver.c:126-135, spread over CTAs):
+// a call with too few tiles to fill the GPU for its k (sched.cu decides,
+// from the whole call's shape) runs on persistent CTAs that take (tile,
+// k-chunk) units from a counter; each chunk stores its sums and the last
+// chunk of a tile to finish adds them in chunk order and runs the epilogue,
+// so the result does not depend on which CTA ran what.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -48,8 +55,168 @@ __device__ __forceinline__ void lds16(double (&d)[2], const double *p) {
   d[0] = v.x; d[1] = v.y;
 }
 
-// SPLIT: the split-K epilogue is compiled in (launched only when splits > 1,
-// so the unsplit kernel keeps its registers for the main loop).
+// One output tile per CTA (block index -> tile, rasterised in groups of 8
+// along M); tiles outside the written triangle exit at once.  Used for
+// every call that is not split along k: a persistent schedule of the same
+// tiles measured no faster (SGEMM 4096^3: 55.8 vs 55.6 TF/s), the tiles'
+// own efficiency, not the last wave, being the limit there.
+template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB,
+          bool PAIR = false>
+__global__ void __launch_bounds__(256, MINB) simt_tile_kernel(SimtGemmArgs<T> p) {
+  constexpr int NT = 256;
+  constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;
+  constexpr int TM = WTM / 4, TN = WTN / 8;
+  // Fragments are 16-byte chunks of CW elements; a thread's chunks are
+  // spaced so that one warp-wide load touches 4 (A) or 8 (B) consecutive
+  // chunks: a single 128-byte wavefront, no bank conflicts.
+  constexpr int CW = 16 / sizeof(T);
+  constexpr int MCH = TM / CW, NCH = TN / CW;
+  constexpr int MSP = 4 * CW, NSP = 8 * CW;  // chunk spacing
+  constexpr int VEC = CW;
+  static_assert(WARPS_M * WARPS_N == 8, "8 warps");
+  static_assert(TM % CW == 0 && TN % CW == 0, "16-byte fragments");
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *As = reinterpret_cast<T *>(smem_raw);
+  T *Bs = As + STAGES * BK * BM;
+
+  // Rasterise tiles in groups of 8 along M for L2 reuse of B panels.
+  const int tiles_m = (p.m + BM - 1) / BM, tiles_n = (p.n + BN - 1) / BN;
+  const int bid = blockIdx.x;
+  constexpr int G = 8;
+  const int group = bid / (G * tiles_n);
+  const int first_m = group * G;
+  const int gsize = min(tiles_m - first_m, G);
+  const int in_group = bid % (G * tiles_n);
+  const int tm = first_m + in_group % gsize, tn = in_group / gsize;
+  const long m0 = (long)tm * BM, n0 = (long)tn * BN;
+
+  // block_is_outside(ji, n0, BN, m0, BM)
+  if (p.ji == MUBLIS_L3_LOWER && n0 >= m0 + BM) return;
+  if (p.ji == MUBLIS_L3_UPPER && n0 + BN <= m0) return;
+
+  long kb = 0, ke = p.k;
+  if (p.jp == MUBLIS_L3_LOWER) kb = max(kb, n0);       // j <= p
+  if (p.jp == MUBLIS_L3_UPPER) ke = min(ke, n0 + BN);  // j >= p
+  if (p.pi == MUBLIS_L3_LOWER) ke = min(ke, m0 + BM);  // p <= i
+  if (p.pi == MUBLIS_L3_UPPER) kb = max(kb, m0);       // p >= i
+  const int kt_begin = (int)(kb / BK);
+  const int kt_end = ke > kb ? (int)((ke + BK - 1) / BK) : kt_begin;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wm = warp % WARPS_M, wn = warp / WARPS_M;
+  const int ty = lane >> 3, tx = lane & 7;
+
+  // PAIR (FP32 only): accumulators as column pairs updated with the packed
+  // sm_100 FMA (__ffma2_rn: two correctly rounded fmaf per instruction), so
+  // the FMA stream takes half the issue slots and the loads and address
+  // arithmetic fit beside it.  Each element's result is that of fmaf.
+  static_assert(!PAIR || (sizeof(T) == 4 && TN % 2 == 0), "pairs are FP32 column pairs");
+  constexpr int TNP = PAIR ? TN / 2 : TN;
+  using Acc = typename std::conditional<PAIR, float2, T>::type;
+  Acc acc[TM][TNP];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TNP; ++j) {
+      if constexpr (PAIR) acc[i][j] = make_float2(0.f, 0.f);
+      else acc[i][j] = T(0);
+    }
+
+  auto load_stage = [&](int stage, int kt) {
+    const T *ga = p.ap + (long)kt * BK * p.lda + m0;
+    const T *gb = p.bp + (long)kt * BK * p.ldb + n0;
+    T *sa = As + stage * BK * BM;
+    T *sb = Bs + stage * BK * BN;
+#pragma unroll
+    for (int c = tid; c < BK * BM / VEC; c += NT) {
+      int row = c / (BM / VEC), col = (c % (BM / VEC)) * VEC;
+      cp_async16(sa + row * BM + col, ga + (long)row * p.lda + col);
+    }
+#pragma unroll
+    for (int c = tid; c < BK * BN / VEC; c += NT) {
+      int row = c / (BN / VEC), col = (c % (BN / VEC)) * VEC;
+      cp_async16(sb + row * BN + col, gb + (long)row * p.ldb + col);
+    }
+  };
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (kt_begin + s < kt_end) load_stage(s, kt_begin + s);
+    cp_async_commit();
+  }
+
+  for (int kt = kt_begin; kt < kt_end; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const int nk = kt + STAGES - 1;
+    if (nk < kt_end) load_stage((nk - kt_begin) % STAGES, nk);
+    cp_async_commit();
+
+    const int st = (kt - kt_begin) % STAGES;
+    const T *sa = As + st * BK * BM + wm * WTM + ty * CW;
+    const T *sb = Bs + st * BK * BN + wn * WTN + tx * CW;
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T af[TM], bf[TN];
+#pragma unroll
+      for (int mc = 0; mc < MCH; ++mc) {
+        T t[CW];
+        lds16(t, sa + kk * BM + mc * MSP);
+#pragma unroll
+        for (int q = 0; q < CW; ++q) af[mc * CW + q] = t[q];
+      }
+#pragma unroll
+      for (int nc = 0; nc < NCH; ++nc) {
+        T t[CW];
+        lds16(t, sb + kk * BN + nc * NSP);
+#pragma unroll
+        for (int q = 0; q < CW; ++q) bf[nc * CW + q] = t[q];
+      }
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TNP; ++j) {
+          if constexpr (PAIR)
+            acc[i][j] = __ffma2_rn(make_float2(af[i], af[i]), make_float2(bf[2 * j], bf[2 * j + 1]),
+                                   acc[i][j]);
+          else
+            acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  // Per row, the TN loads of C are issued before the stores (one memory
+  // round trip per row rather than per element).
+  const T alpha = p.alpha, beta = p.beta;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const long gi = m0 + wm * WTM + (i / CW) * MSP + ty * CW + (i % CW);
+    if (gi >= p.m) continue;
+    T cv[TN];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + wn * WTN + (j / CW) * NSP + tx * CW + (j % CW);
+      const bool in = gj < p.n && b200_rel(p.ji, gj, gi);
+      cv[j] = in && beta != T(0) ? p.c[gi * p.rs_c + gj * p.cs_c] : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long gj = n0 + wn * WTN + (j / CW) * NSP + tx * CW + (j % CW);
+      if (gj >= p.n || !b200_rel(p.ji, gj, gi)) continue;
+      T v;
+      if constexpr (PAIR) v = alpha * ((j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x);
+      else v = alpha * acc[i][j];
+      if (beta != T(0)) v = fma(beta, cv[j], v);
+      p.c[gi * p.rs_c + gj * p.cs_c] = v;
+    }
+  }
+}
+
+
+// Persistent CTAs over (tile, k-chunk) units for split-K calls (SPLIT:
+// the split epilogue compiled in).
 template <typename T, int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, int MINB,
           bool PAIR = false, bool SPLIT = false>
 __global__ void __launch_bounds__(256, MINB) simt_gemm_kernel(SimtGemmArgs<T> p) {
@@ -315,7 +482,7 @@ template <typename T, int BM, int BN, int WM, int WN, int ST, int MINB, bool PAI
 int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol) {
   constexpr int BK = SimtConfig<T>::BK;
   constexpr int E = (BM / WM / 4) * (BN / WN / 8);  // accumulators per thread
-  auto kern = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR, false>;
+  auto kern = simt_tile_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR>;
   auto kern_split = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR, true>;
   const size_t smem = (size_t)ST * BK * (BM + BN) * sizeof(T);
   static int per_sm = 0;
@@ -328,12 +495,13 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
   const long tiles = b200_ceil_div(a0.m, BM) * b200_ceil_div(a0.n, BN);
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL / 16) return b200_set_error(B200_EINVAL, "gemm: too many tiles");
-  // MUBLIS_B200_SIMT_PERSIST=0 keeps one tile per CTA for every call (tuning).
-  static const bool persist = [] {
-    const char *e = getenv("MUBLIS_B200_SIMT_PERSIST");
-    return !(e && !strcmp(e, "0"));
-  }();
-  if (!pol || !persist) {  // one tile per CTA, nothing allocated
+  // Split-K from the whole call's shape (a split unit's 64 KB of partial
+  // sums cost about 4 k-block times); unsplit calls take one tile per CTA.
+  const long slots = (long)per_sm * b200_sm_count();
+  const b200_tile_domain_t dom = {a0.jp, a0.ji, a0.pi};
+  const int S = pol ? b200_split_for(pol->m_full, pol->n_full, a0.k, BM, BN, BK, dom, slots, 4.0)
+                    : 1;
+  if (S == 1) {  // nothing allocated
     B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
     kern<<<(unsigned)tiles, 256, smem, s>>>(a0);
     B200_LAUNCH_CHECK();
@@ -341,10 +509,8 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
   }
 
   // Persistent CTAs over the tiles that write (heaviest first), each tile's
-  // k range cut into S chunks chosen from the whole call's shape.
+  // k range cut into S chunks.
   SimtGemmArgs<T> a = a0;
-  const long slots = (long)per_sm * b200_sm_count();
-  const b200_tile_domain_t dom = {a.jp, a.ji, a.pi};
   std::vector<int2> list;
   const bool restricted = a.jp != MUBLIS_L3_ALL || a.ji != MUBLIS_L3_ALL || a.pi != MUBLIS_L3_ALL;
   long ntiles = tiles;
@@ -353,8 +519,6 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
     ntiles = (long)list.size();
     if (ntiles == 0) return B200_OK;
   }
-  // A split unit's 64 KB of partial sums cost about 4 k-block times.
-  const int S = b200_split_for(pol->m_full, pol->n_full, a.k, BM, BN, BK, dom, slots, 4.0);
   const long units = ntiles * S;
   const size_t ints = sizeof(int) * (size_t)(1 + ntiles);
   const size_t list_bytes = sizeof(int2) * list.size();
@@ -376,8 +540,7 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
     a.splits = S;
     a.partials = S > 1 ? (T *)(scratch + off_part) : nullptr;
     B200ProfScope prof(sizeof(T) == 4 ? "simt_sgemm" : "simt_dgemm", s);
-    if (S > 1) kern_split<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
-    else kern<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
+    kern_split<<<(unsigned)std::min(units, slots), 256, smem, s>>>(a);
     if (cudaGetLastError() != cudaSuccess) st = b200_set_error(B200_ECUDA, "gemm: launch failed");
   }
   b200_free(scratch);

@@ -337,22 +337,65 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
     }
   };
 
-  // acc[q] -= A_blk X_d: the packed block times the solved block d.
-  auto update = [&](int q, const T *ablk, const T *xd) {
+  // acc[q] -= A_rb,d X_d for row blocks rb = warp + 8 q, q = Q0 .. 3, all in
+  // one unrolled sequence so that the blocks' independent MMA / FMA chains
+  // interleave; X_d's operand fragments (xb / xr) are loaded once per step.
+  // Row blocks past the leaf (rb >= nb) multiply a zero block instead of
+  // reading past the segment.
+  using XFrag = typename std::conditional<F64, double[4][4], float[LB]>::type;
+  auto update_from = [&](auto q0c, const T *sg, int d, const XFrag &xf) {
+    constexpr int Q0 = decltype(q0c)::value;
     if constexpr (F64) {
-      const double2 *af = (const double2 *)ablk;
 #pragma unroll
       for (int ks = 0; ks < 4; ++ks) {
-        const double2 a = af[ks * 32 + lane];
+        double2 a[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          dmma(acc[q][j], -a.x, -a.y, xd[(4 * ks + t) * XS_LD + 8 * j + g]);
+        for (int q = Q0; q < 4; ++q) {
+          const int rb = warp + 8 * q;
+          a[q] = rb < nb ? ((const double2 *)(sg + (rb - d - 1) * BLK))[ks * 32 + lane]
+                         : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = Q0; q < 4; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc[q][j], -a[q].x, -a[q].y, xf[ks][j]);
       }
     } else {
 #pragma unroll
       for (int kk = 0; kk < LB; ++kk) {
-        const float xv = -xd[kk * XS_LD + lane];
-        const float4 *col = (const float4 *)(ablk + kk * LB);  // column kk of the block
+        const float xv = xf[kk];
+#pragma unroll
+        for (int q = Q0; q < 4; ++q) {
+          const int rb = warp + 8 * q;
+          if (rb >= nb) continue;
+          const float4 *col = (const float4 *)(sg + (rb - d - 1) * BLK + kk * LB);
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const float4 a = col[v];
+            acc[q][2 * v] =
+                __ffma2_rn(make_float2(a.x, a.y), make_float2(xv, xv), acc[q][2 * v]);
+            acc[q][2 * v + 1] =
+                __ffma2_rn(make_float2(a.z, a.w), make_float2(xv, xv), acc[q][2 * v + 1]);
+          }
+        }
+      }
+    }
+  };
+  // The owner's block d + 1 alone (block 0 of the segment).
+  auto update_one = [&](int q, const T *sg, const XFrag &xf) {
+    if constexpr (F64) {
+      const double2 *af = (const double2 *)sg;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const double2 a = af[ks * 32 + lane];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[q][j], -a.x, -a.y, xf[ks][j]);
+      }
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < LB; ++kk) {
+        const float xv = xf[kk];
+        const float4 *col = (const float4 *)(sg + kk * LB);
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           const float4 a = col[v];
@@ -376,6 +419,16 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
       if (tid == 0 && d + 2 <= nb - 2) issue(d + 2);
       const T *sg = seg + (d % RING) * SEG_MAX;
       const T *xd = xs + (d & 1) * LB * XS_LD;
+      XFrag xf;
+      if constexpr (F64) {
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) xf[ks][j] = xd[(4 * ks + t) * XS_LD + 8 * j + g];
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < LB; ++kk) xf[kk] = -xd[kk * XS_LD + lane];
+      }
       // (q runs over compile-time values so the accumulators stay in
       // registers.)  The owner of block d + 1 goes first: its update and
       // solve are the step's critical path.
@@ -383,15 +436,19 @@ __global__ void __launch_bounds__(THREADS, 1) trsm_leaf_kernel(const __grid_cons
       for (int q = 0; q < 4; ++q) {
         const int rb = warp + 8 * q;
         if (rb == d + 1) {
-          update(q, sg, xd);
+          update_one(q, sg, xf);
           solve(q, sg + (nb - 1 - d) * BLK, xs + ((d + 1) & 1) * LB * XS_LD);
         }
       }
       write_block(d, xd);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int rb = warp + 8 * q;
-        if (rb > d + 1 && rb < nb) update(q, sg + (rb - d - 1) * BLK, xd);
+      // This warp's blocks below d + 1: q >= qlo.
+      const int qlo = d + 1 - warp < 0 ? 0 : (d + 1 - warp) / 8 + 1;
+      switch (qlo) {
+        case 0: update_from(std::integral_constant<int, 0>(), sg, d, xf); break;
+        case 1: update_from(std::integral_constant<int, 1>(), sg, d, xf); break;
+        case 2: update_from(std::integral_constant<int, 2>(), sg, d, xf); break;
+        case 3: update_from(std::integral_constant<int, 3>(), sg, d, xf); break;
+        default: break;
       }
     }
     if (d + 1 == nb) {
