@@ -8,7 +8,11 @@
 //   * recursive halving: solve the top half, update the bottom half with one
 //     GEMM (k = half the order, so it runs at GEMM speed), solve the bottom
 //     half (upper: mirror image);
-//   * leaves are the 512 x 512 (1024 x 1024 for large solves) diagonal
+//   * FP64 leaves (512 rows) are solved by the fused GEMMTRSM kernel
+//     (trsm_leaf.cu): diagonal 16 x 16 blocks in shared memory, the updates
+//     between them on the FP64 tensor pipe, every right-hand side of the
+//     chain in one launch;
+//   * FP32 leaves are the 512 x 512 (1024 x 1024 for large solves) diagonal
 //     blocks, inverted up front: one launch inverts every 64 x 64 diagonal
 //     block by substitution against the reciprocal diagonal (computed once
 //     and multiplied -- never divided -- as the reference does), then
@@ -45,14 +49,21 @@ constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
 // n >= 2048.
 int leaf_order(long m, long n) { return m >= 4096 && n >= 2048 ? 1024 : 512; }
 
-// Solves use the fused leaf kernel (trsm_leaf.cu) unless
-// MUBLIS_B200_TRSM=inverse selects the inverted-diagonal-block products.
-bool fused_leaves() {
-  static const bool on = [] {
+// Leaves: FP64 solves use the fused leaf kernel (trsm_leaf.cu), FP32 solves
+// the inverted diagonal blocks applied as products; MUBLIS_B200_TRSM=fused /
+// inverse selects one for both.  Measured at n = 4096 (device operands):
+// DTRSM 22.4 TF/s fused vs 20.3 inverse (the leaf's updates run on the FP64
+// tensor pipe, and it executes the triangle's flops only, not the 1.25 to 2x
+// of a product with the inverse); STRSM 31.0 fused vs 33.3 inverse (FP32 has
+// no tensor-pipe form, and the inverse products run at the SIMT GEMM's rate).
+bool fused_leaves(int dtype) {
+  static const int forced = [] {
     const char *e = getenv("MUBLIS_B200_TRSM");
-    return !(e && !strcmp(e, "inverse"));
+    if (e && !strcmp(e, "inverse")) return 0;
+    if (e && !strcmp(e, "fused")) return 1;
+    return -1;
   }();
-  return on;
+  return forced >= 0 ? forced == 1 : dtype == B200_F64;
 }
 
 // One CTA per LEAF block: thread j computes column j of the inverse of the
@@ -327,7 +338,7 @@ int build_leaves(const b200_trsm_desc_t *d, TrsmPrep *p) {
 
 template <typename T>
 int build_inverse(const b200_trsm_desc_t *d, TrsmPrep *p) {
-  if (fused_leaves()) return build_leaves(d, p);
+  if (fused_leaves(d->dtype)) return build_leaves(d, p);
   cudaStream_t s = b200_cur_stream();
   T *inv = nullptr, *tmp = nullptr;
   const long big = leaf_order(d->m, d->policy_n > 0 ? d->policy_n : d->n);

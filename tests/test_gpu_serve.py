@@ -27,7 +27,7 @@ def declare_server(lib):
     return lib
 
 
-def make_calls(torch, count, seed):
+def make_calls(torch, count, seed, large=(768, 1024)):
     rng = np.random.default_rng(seed)
     calls = []
     for q in range(count):
@@ -35,7 +35,7 @@ def make_calls(torch, count, seed):
         if rng.random() < 0.85:
             n1, n2, n3 = (int(x) for x in np.floor(np.exp(rng.uniform(np.log(32), np.log(257), 3))))
         else:
-            n1 = n2 = n3 = int(rng.choice([768, 1024]))
+            n1 = n2 = n3 = int(rng.choice(list(large)))
         dt = torch.float32 if kind[0] == "s" else torch.float64
         if kind.endswith("gemm"):
             m, n, k = n1, n2, n3
@@ -74,13 +74,18 @@ def issue(lib, c):
                         p(o[0]), c["m"], p(o[1]), c["m"])
 
 
-def test_results_are_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("forms", ["plain", "auto"])
+def test_results_are_the_same_alone_and_in_the_mix(forms):
+    """forms "auto": the large requests run the tensor-core forms the policy
+    picks (bf16x6 for FP32 from 512, the modular Ozaki form for FP64 from
+    2048^2), alone and in the mix."""
     torch = pytest.importorskip("torch")
     lib = declare_server(mb.load())
     assert lib.mublis_b200_init() == 0
     for p in (b"s", b"d"):
-        lib.mublis_b200_set_form(p, b"plain")
-    calls = make_calls(torch, 96, seed=2)
+        lib.mublis_b200_set_form(p, forms.encode())
+    calls = make_calls(torch, 96, seed=2,
+                       large=(768, 1024) if forms == "plain" else (768, 1024, 2048))
     out_idx = lambda c: 1 if c["kind"] in ("ssyrk", "dtrsm") else 2  # noqa: E731
     initial = [c["ops"][out_idx(c)].clone() for c in calls]
 
@@ -95,8 +100,9 @@ def test_results_are_the_same_alone_and_in_the_mix():
     torch.cuda.synchronize()
 
     # in the mix: 16 host threads through the attached server
+    # Forms left to the library default set above (NULL in the config).
     cfg = ServerConfig(hbm_budget_bytes=8 << 30, streams=4, batch_window_us=200,
-                       small_max_dim=512, max_batch=4096, sform=b"plain", dform=b"plain")
+                       small_max_dim=512, max_batch=4096, sform=None, dform=None)
     srv = ctypes.c_void_p()
     assert lib.mublis_b200_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 0
     assert lib.mublis_b200_server_attach(srv) == 0
@@ -122,6 +128,8 @@ def test_results_are_the_same_alone_and_in_the_mix():
     finally:
         lib.mublis_b200_server_attach(None)
         lib.mublis_b200_server_destroy(srv)
+        for p in (b"s", b"d"):
+            lib.mublis_b200_set_form(p, b"plain")
     torch.cuda.synchronize()
 
     assert st.completed == len(calls)
