@@ -482,8 +482,30 @@ int b200_column_pipeline(const b200_colpipe_t *p) {
     const int npan =
         b200_colpipe_panels_min(p->ncols, 1ull << 40, p->panel_min > 0 ? p->panel_min : 1024);
     const long w0 = b200_round_up(b200_ceil_div(p->ncols, npan < 1 ? 1 : npan), 128);
-    for (long j0 = 0; j0 < p->ncols && np < B200_COLPIPE_MAX_PANELS; j0 += w0, ++np)
-      start[np] = j0, width[np] = p->ncols - j0 < w0 ? p->ncols - j0 : w0;
+    // Half-width first and last panels: the first computation starts after
+    // a smaller copy-in, and the last one (and its copy back, which nothing
+    // overlaps) is shorter.  MUBLIS_B200_PIPE_EDGES=0 keeps even panels.
+    static const bool edges = [] {
+      const char *e = getenv("MUBLIS_B200_PIPE_EDGES");
+      return !(e && !strcmp(e, "0"));
+    }();
+    const long half = b200_round_up(w0 / 2, 128);
+    // (Calls whose panels must stay wide -- TRSM / TRMM, panel_min 2048 --
+    // keep even panels.)
+    if (edges && p->panel_min <= 1024 && npan >= 2 && half < w0 &&
+        npan + 1 <= B200_COLPIPE_MAX_PANELS && (p->ncols - half) / 128 * 128 > half) {
+      start[0] = 0, width[0] = half, np = 1;
+      // The last panel starts on a multiple of 128, like every other one.
+      const long last = (p->ncols - half) / 128 * 128;
+      for (long j0 = half; j0 < last && np < B200_COLPIPE_MAX_PANELS - 1; ++np) {
+        const long wq = last - j0 < w0 ? last - j0 : w0;
+        start[np] = j0, width[np] = wq, j0 += wq;
+      }
+      start[np] = last, width[np] = p->ncols - last, ++np;
+    } else {
+      for (long j0 = 0; j0 < p->ncols && np < B200_COLPIPE_MAX_PANELS; j0 += w0, ++np)
+        start[np] = j0, width[np] = p->ncols - j0 < w0 ? p->ncols - j0 : w0;
+    }
   }
   if (p->nstreams < 0 || p->nstreams > B200_COLPIPE_MAX_STREAMS)
     return b200_set_error(B200_EINVAL, "pipeline: too many streamed operands");

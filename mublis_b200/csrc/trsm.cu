@@ -267,6 +267,10 @@ int trsm_rec(const Chains &ch, const TrsmPrep *prep, long r0, long r1) {
     return for_each_chain(ch, [&](const b200_trsm_desc_t &d) {
       T *b = (T *)d.b;
       b200_l3_desc_t g = plain_gemm_desc(d.dtype, B200_FORM_PLAIN, 0);
+      // The whole call's n: a column panel (or chain) of a larger solve then
+      // schedules (splits) the product as the whole call would, so every
+      // column gets the same bits either way.
+      g.policy_n = d.policy_n;
       g.product.domain.pi = lower ? MUBLIS_L3_LOWER : MUBLIS_L3_UPPER;
       g.product.a.struc = MUBLIS_STRUC_TRIANGULAR;
       g.product.a.uplo = d.uplo;
