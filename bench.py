@@ -764,6 +764,9 @@ def main():
                     help="run only the TRSM/TRMM side x uplo x transpose study")
     ap.add_argument("--only-grouped", action="store_true",
                     help="run only config 4's SGEMMs as direct grouped calls (profiler captures)")
+    ap.add_argument("--only-trsm", default=None, choices=["s", "d"],
+                    help="run only two TRSMs of order --n with --n right-hand sides "
+                         "(left, lower, non-unit; profiler captures of the TRSM kernels)")
     ap.add_argument("--only-timed", action="store_true",
                     help="warm-up + timed steps only (for profiler launch lists)")
     args = ap.parse_args()
@@ -796,6 +799,23 @@ def main():
     if args.only_sides:
         if rank == 0:
             print(json.dumps({"sides_tflops": sides_study(torch, lib, args.n), "n": args.n}))
+        return
+
+    if args.only_trsm:
+        if rank == 0:
+            p = args.only_trsm
+            dt = torch.float32 if p == "s" else torch.float64
+            n = args.n
+            a = torch.empty(n, n, dtype=dt, device="cuda")
+            getattr(lib, f"mublis_b200_fill_{p}")(ctypes.c_void_p(a.data_ptr()), n, n, n, 0, 0, 0)
+            a.div_(n)
+            a.diagonal().add_(1.5)
+            b = torch.rand(n, n, dtype=dt, device="cuda")
+            fn = getattr(lib, f"mublis_{p}trsm")
+            for _ in range(2):
+                mb.check(fn(0, 1, 0, 0, n, n, 1.0, a.data_ptr(), 1, n, b.data_ptr(), 1, n), lib)
+            torch.cuda.synchronize()
+            print(json.dumps({"trsm": p, "n": n, "ok": True}))
         return
 
     if args.only_grouped:
