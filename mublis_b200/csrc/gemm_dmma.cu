@@ -32,7 +32,7 @@ constexpr int CONSUMERS = 8;  // 2 (m) x 4 (n) warps of 64 x 32
 constexpr int THREADS = (CONSUMERS + 1) * 32;
 constexpr int TILE_BYTES = BM * BK * 8;  // 16 KB per operand per k-block
 constexpr int STAGE_BYTES = 2 * TILE_BYTES;
-constexpr int SMEM = STAGES * STAGE_BYTES + 128;
+constexpr int SMEM = STAGES * STAGE_BYTES + 128 + 1024;  // + alignment slack for swizzled tiles
 constexpr int QUAD_DOUBLES = 8 * 32 * 2;  // one k-quad of a 128-row strip
 
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
@@ -91,9 +91,22 @@ __device__ __forceinline__ void chunk_range(int chunk, int S, int &kt0, int &kt1
   kt0 = b;
 }
 
+// Offset (doubles) of element (r, e) of a 128-row x 16 tile stored with the
+// 16 innermost: 128-byte rows whose 16-byte chunks are XOR-swizzled by the
+// row's low three bits (the TMA 128-byte swizzle).
+__device__ __forceinline__ int swz16(int r, int e) {
+  return r * 16 + ((((e >> 1) ^ r) & 7) << 1) + (e & 1);
+}
+
+// DIRECT: operands come as 2-D TMA tiles of the caller's matrices (AK / BK:
+// k innermost, swizzled [128][16]; else m / n innermost, [16][128]); else
+// from PACK_FRAG64 panels by 1-D bulk copies.
+template <bool DIRECT, bool AK, bool BK>
 __global__ void __launch_bounds__(THREADS, 1)
     dmma_gemm_kernel(const __grid_constant__ DmmaGemmArgs p) {
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // Swizzled TMA tiles need 1024-byte aligned destinations.
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
   uint64_t *empty = full + STAGES;
   volatile int *abort_flag = (volatile int *)(empty + STAGES);
@@ -125,8 +138,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       tile_coords(p, u / S, tm, tn);
       if (!tile_krange(p, tm, tn, kt0, kt1)) continue;
       chunk_range(u % S, S, kt0, kt1);
-      const double *ga = p.ap + (long)tm * p.kq * 2 * 8 * 32;
-      const double *gb = p.bp + (long)tn * p.kq * 2 * 8 * 32;
+      const double *ga = DIRECT ? nullptr : p.ap + (long)tm * p.kq * 2 * 8 * 32;
+      const double *gb = DIRECT ? nullptr : p.bp + (long)tn * p.kq * 2 * 8 * 32;
       for (int kt = kt0; kt < kt1; ++kt) {
         if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err, p.wait_ns)) {
           ok = false;
@@ -134,9 +147,24 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
         unsigned char *dst = smem + stage * STAGE_BYTES;
-        tc::bulk_load_1d(dst, ga + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES, &full[stage]);
-        tc::bulk_load_1d(dst + TILE_BYTES, gb + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES,
-                         &full[stage]);
+        if constexpr (DIRECT) {
+          // The k-block's pair and its k within the pair; the coordinates
+          // are multiples of 16 (k) and 128 (m, n), as TMA wants.
+          int kl = kt * BK, q = 0;
+          if (p.npairs == 2 && kl >= p.kpair) {
+            q = 1;
+            kl -= (int)p.kpair;
+          }
+          const int m0 = tm * BM, n0 = tn * BN;
+          if (AK) tc::tma_load_2d(dst, &p.ta[q], &full[stage], kl, m0);
+          else tc::tma_load_2d(dst, &p.ta[q], &full[stage], m0, kl);
+          if (BK) tc::tma_load_2d(dst + TILE_BYTES, &p.tb[q], &full[stage], kl, n0);
+          else tc::tma_load_2d(dst + TILE_BYTES, &p.tb[q], &full[stage], n0, kl);
+        } else {
+          tc::bulk_load_1d(dst, ga + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES, &full[stage]);
+          tc::bulk_load_1d(dst + TILE_BYTES, gb + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES,
+                           &full[stage]);
+        }
         ++issued;
         if (++stage == STAGES) { stage = 0; phase ^= 1; }
       }
@@ -169,21 +197,48 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int kt = kt0; kt < kt1; ++kt) {
       const int wok = tc::mbar_wait(&full[stage], phase, abort_flag, p.err, p.wait_ns);
       if (!__all_sync(0xffffffffu, wok)) return;
-      const double2 *As = (const double2 *)(smem + stage * STAGE_BYTES) + wm * 4 * 32 + lane;
-      const double2 *Bs =
-          (const double2 *)(smem + stage * STAGE_BYTES + TILE_BYTES) + wn * 2 * 32 + lane;
+      if constexpr (DIRECT) {
+        // Fragments straight from the TMA tiles: a = rows ib*16 + g (+8),
+        // k = 4 ks + t of op(A); b = k = 4 ks + t, column jb*8 + g of op(B).
+        const double *At = (const double *)(smem + stage * STAGE_BYTES);
+        const double *Bt = (const double *)(smem + stage * STAGE_BYTES + TILE_BYTES);
 #pragma unroll
-      for (int ks = 0; ks < BK / 4; ++ks) {
-        double2 a[4], b[2];
+        for (int ks = 0; ks < BK / 4; ++ks) {
+          const int e = 4 * ks + t;
+          double a0[4], a1[4], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[(ks * 8 + i) * 32];
+          for (int i = 0; i < 4; ++i) {
+            const int r = (wm * 4 + i) * 16 + g;
+            a0[i] = AK ? At[swz16(r, e)] : At[e * BM + r];
+            a1[i] = AK ? At[swz16(r + 8, e)] : At[e * BM + r + 8];
+          }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) b[j] = Bs[(ks * 8 + j) * 32];
+          for (int j = 0; j < 4; ++j) {
+            const int c = (wn * 4 + j) * 8 + g;
+            b[j] = BK ? Bt[swz16(c, e)] : Bt[e * BN + c];
+          }
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+          for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            dmma(acc[i][j], a[i].x, a[i].y, (j & 1) ? b[j >> 1].y : b[j >> 1].x);
+            for (int j = 0; j < 4; ++j) dmma(acc[i][j], a0[i], a1[i], b[j]);
+        }
+      } else {
+        const double2 *As = (const double2 *)(smem + stage * STAGE_BYTES) + wm * 4 * 32 + lane;
+        const double2 *Bs =
+            (const double2 *)(smem + stage * STAGE_BYTES + TILE_BYTES) + wn * 2 * 32 + lane;
+#pragma unroll
+        for (int ks = 0; ks < BK / 4; ++ks) {
+          double2 a[4], b[2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) a[i] = As[(ks * 8 + i) * 32];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) b[j] = Bs[(ks * 8 + j) * 32];
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              dmma(acc[i][j], a[i].x, a[i].y, (j & 1) ? b[j >> 1].y : b[j >> 1].x);
+        }
       }
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&empty[stage]);
@@ -263,22 +318,33 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+template <bool DIRECT, bool AK, bool BK>
+int launch_variant(const DmmaGemmArgs &a, int grid, cudaStream_t s) {
+  auto kern = dmma_gemm_kernel<DIRECT, AK, BK>;
+  static bool configured = false;
+  if (!configured) {
+    B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    configured = true;
+  }
+  B200ProfScope prof("dmma_dgemm", s);
+  kern<<<grid, THREADS, SMEM, s>>>(a);
+  B200_LAUNCH_CHECK();
+  return B200_OK;
+}
+
 }  // namespace
 
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s) {
   const long tiles = (a.tile_list ? a.ntiles : (long)a.tiles_m * a.tiles_n) * a.splits;
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL) return b200_set_error(B200_EINVAL, "dgemm: too many tiles");
-  static bool configured = false;
-  if (!configured) {
-    B200_CUDA_TRY(
-        cudaFuncSetAttribute(dmma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-    configured = true;
-  }
   const int sms = b200_sm_count();
   const int grid = (int)(tiles < sms ? tiles : sms);
-  B200ProfScope prof("dmma_dgemm", s);
-  dmma_gemm_kernel<<<grid, THREADS, SMEM, s>>>(a);
-  B200_LAUNCH_CHECK();
-  return B200_OK;
+  if (!a.direct) return launch_variant<false, false, false>(a, grid, s);
+  if (a.a_kcontig) {
+    return a.b_kcontig ? launch_variant<true, true, true>(a, grid, s)
+                       : launch_variant<true, true, false>(a, grid, s);
+  }
+  return a.b_kcontig ? launch_variant<true, false, true>(a, grid, s)
+                     : launch_variant<true, false, false>(a, grid, s);
 }

@@ -1,6 +1,7 @@
 // kernels.cuh -- launchers shared between the CUDA translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -207,6 +208,16 @@ struct DmmaGemmArgs {
   int splits = 1;
   int *arrivals = nullptr;
   double *partials = nullptr;
+  // Direct operand loads (no pack pass): 2-D TMA tiles read straight from
+  // the caller's op(A) and op(B), one tensor map per operand and pair (a
+  // SYR2K's two pairs split k at kpair, a multiple of the k-block).
+  // a_kcontig / b_kcontig: the operand's unit stride runs along k (tiles
+  // then land 128-byte swizzled, k innermost); otherwise along m / n.
+  int direct = 0;
+  int a_kcontig = 0, b_kcontig = 0;
+  int npairs = 1;
+  long kpair = 0;
+  CUtensorMap ta[2], tb[2];
 };
 int launch_dmma_gemm(const DmmaGemmArgs &a, cudaStream_t s);
 constexpr int B200_DMMA_TILE = 128, B200_DMMA_BK = 16;

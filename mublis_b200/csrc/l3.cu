@@ -8,6 +8,7 @@
 // triangle tiles through a temporary (:192-234).  Here each operand is packed
 // once for the whole call (one HBM pass, pack.cu) and the contraction kernel
 // tiles the entire output on the device.
+#include <cstdint>
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
@@ -81,19 +82,113 @@ bool use_dmma() {
   return on;
 }
 
+// A strided FP64 view (rows x cols, element (i, j) at x + i rs + j cs) as a
+// TMA source: one stride must be 1 and the other a positive multiple of 2
+// elements (16 bytes) at least the unit-stride extent, the base 16-byte
+// aligned.  *first_contig: the unit stride runs along the rows index.
+bool tma_view_ok(const void *x, long rs, long cs, long rows, long cols, bool *rows_contig) {
+  if (((uintptr_t)x & 15) != 0 || rows <= 0 || cols <= 0) return false;
+  if (rs == 1 && cs >= rows && cs % 2 == 0) {
+    *rows_contig = true;
+    return true;
+  }
+  if (cs == 1 && rs >= cols && rs % 2 == 0) {
+    *rows_contig = false;
+    return true;
+  }
+  return false;
+}
+
+// Byte interval [lo, hi] spanned by a view with non-negative strides.
+void view_span(const void *x, long rs, long cs, long rows, long cols, uintptr_t *lo,
+               uintptr_t *hi) {
+  *lo = (uintptr_t)x;
+  *hi = (uintptr_t)x + sizeof(double) * ((rows - 1) * rs + (cols - 1) * cs + 1) - 1;
+}
+
+// The FP64 tensor-pipe kernel can read op(A) and op(B) straight from the
+// caller's memory (2-D TMA tiles) instead of packed panels when no element
+// needs changing on the way: general operands, no jp / pi mask, every pair
+// with the same orientation, a SYR2K's pairs meeting on a k-block boundary,
+// and C overlapping no operand (an in-place product must read its operand
+// before it is overwritten, which only a copy guarantees).
+// MUBLIS_B200_DIRECT=0 keeps the pack pass for every call.
+bool dmma_direct(const b200_l3_desc_t *d, DmmaGemmArgs *g) {
+  static const bool on = [] {
+    const char *e = getenv("MUBLIS_B200_DIRECT");
+    return !(e && !strcmp(e, "0"));
+  }();
+  const mublis_l3_product_t &pr = d->product;
+  if (!on || pr.a.struc != MUBLIS_STRUC_GENERAL || pr.b.struc != MUBLIS_STRUC_GENERAL ||
+      pr.domain.jp != MUBLIS_L3_ALL || pr.domain.pi != MUBLIS_L3_ALL)
+    return false;
+  if (d->npairs == 2 && d->k % B200_DMMA_BK != 0) return false;
+  if (d->rs_c < 0 || d->cs_c < 0) return false;
+  uintptr_t clo, chi;
+  view_span(d->c, d->rs_c, d->cs_c, d->m, d->n, &clo, &chi);
+  bool a_mc = false, b_kc = false;
+  for (int t = 0; t < d->npairs; ++t) {
+    bool ac, bc;
+    if (!tma_view_ok(d->a[t], d->rs_a[t], d->cs_a[t], d->m, d->k, &ac) ||
+        !tma_view_ok(d->b[t], d->rs_b[t], d->cs_b[t], d->k, d->n, &bc))
+      return false;
+    if (t == 0) {
+      a_mc = ac;
+      b_kc = bc;
+    } else if (ac != a_mc || bc != b_kc) {
+      return false;
+    }
+    uintptr_t lo, hi;
+    view_span(d->a[t], d->rs_a[t], d->cs_a[t], d->m, d->k, &lo, &hi);
+    if (lo <= chi && clo <= hi) return false;
+    view_span(d->b[t], d->rs_b[t], d->cs_b[t], d->k, d->n, &lo, &hi);
+    if (lo <= chi && clo <= hi) return false;
+  }
+  // Tensor maps: op(A) tile 128 (m) x 16 (k), op(B) tile 16 (k) x 128 (n);
+  // k innermost tiles are 16 doubles = 128 bytes, 128-byte swizzled.
+  memset(g->ta, 0, sizeof g->ta);
+  memset(g->tb, 0, sizeof g->tb);
+  for (int t = 0; t < d->npairs; ++t) {
+    int st = a_mc ? b200_make_tmap_f64(&g->ta[t], d->a[t], d->m, d->k, d->cs_a[t],
+                                       B200_DMMA_TILE, B200_DMMA_BK, 0)
+                  : b200_make_tmap_f64(&g->ta[t], d->a[t], d->k, d->m, d->rs_a[t],
+                                       B200_DMMA_BK, B200_DMMA_TILE, 1);
+    if (st == B200_OK)
+      st = b_kc ? b200_make_tmap_f64(&g->tb[t], d->b[t], d->k, d->n, d->cs_b[t], B200_DMMA_BK,
+                                     B200_DMMA_TILE, 1)
+                : b200_make_tmap_f64(&g->tb[t], d->b[t], d->n, d->k, d->rs_b[t],
+                                     B200_DMMA_TILE, B200_DMMA_BK, 0);
+    if (st != B200_OK) {
+      b200_set_error(B200_OK, "");  // not an error: fall back to the pack pass
+      return false;
+    }
+  }
+  g->direct = 1;
+  g->a_kcontig = !a_mc;
+  g->b_kcontig = b_kc;
+  g->npairs = d->npairs;
+  g->kpair = d->k;
+  return true;
+}
+
 int run_dmma(const b200_l3_desc_t *d) {
   cudaStream_t s = b200_cur_stream();
   const long ktot = (long)d->k * d->npairs;
   const long mpad = b200_round_up(d->m, B200_DMMA_TILE);
   const long npad = b200_round_up(d->n, B200_DMMA_TILE);
   const long kpad = b200_round_up(ktot, B200_DMMA_BK);
+  DmmaGemmArgs g;
+  const bool direct = dmma_direct(d, &g);
   void *ap = nullptr, *bp = nullptr;
-  B200_TRY(b200_alloc(&ap, sizeof(double) * mpad * kpad));
-  int st = b200_alloc(&bp, sizeof(double) * npad * kpad);
-  if (st == B200_OK) {
-    PackOut oa{ap, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
-    PackOut ob{bp, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
-    st = pack_pairs<double>(d, oa, mpad, ob, npad, kpad, s);
+  int st = B200_OK;
+  if (!direct) {
+    B200_TRY(b200_alloc(&ap, sizeof(double) * mpad * kpad));
+    st = b200_alloc(&bp, sizeof(double) * npad * kpad);
+    if (st == B200_OK) {
+      PackOut oa{ap, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
+      PackOut ob{bp, kpad, 0, PACK_FRAG64, PACK_COPY, 1, nullptr};
+      st = pack_pairs<double>(d, oa, mpad, ob, npad, kpad, s);
+    }
   }
   // Restricted domains: list the tiles that write (ji) with their k-range
   // (jp, pi), heaviest first (the host twin of the kernel's tile_krange).
@@ -153,7 +248,6 @@ int run_dmma(const b200_l3_desc_t *d) {
       st = b200_set_error(B200_ECUDA, "dgemm: split-K counters");
   }
   if (st == B200_OK && (list == nullptr || ntiles > 0)) {
-    DmmaGemmArgs g;
     g.ap = (const double *)ap;
     g.bp = (const double *)bp;
     g.kq = kpad / 4;

@@ -280,5 +280,11 @@ __host__ __device__ constexpr uint32_t idesc_s8(int m, int n) {
 int b200_make_tmap(CUtensorMap *map, const void *base, int is_bf16, long k, long rows,
                    int box_k, int box_rows, int swz);
 
+// Host: encode a 2-D FP64 tensor map over a strided matrix: `inner`
+// elements along the unit-stride dimension, `outer` along the other (outer
+// stride in elements), box box_inner x box_outer, 128-byte swizzle or none.
+int b200_make_tmap_f64(CUtensorMap *map, const void *base, long inner, long outer,
+                       long outer_stride, int box_inner, int box_outer, int swizzle128);
+
 // Device error word (mapped host memory) kernels report timeouts into.
 int *b200_device_error_word();

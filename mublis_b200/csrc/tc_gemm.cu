@@ -94,6 +94,22 @@ int b200_make_tmap(CUtensorMap *map, const void *base, int is_bf16, long k, long
   return B200_OK;
 }
 
+int b200_make_tmap_f64(CUtensorMap *map, const void *base, long inner, long outer,
+                       long outer_stride, int box_inner, int box_outer, int swizzle128) {
+  std::call_once(g_encode_once, init_encode);
+  if (!g_encode) return b200_set_error(B200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)(outer_stride * (long)sizeof(double))};
+  cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return b200_set_error(B200_ECUDA, "cuTensorMapEncodeTiled (f64) failed");
+  return B200_OK;
+}
+
 // ---- shared tile walk ---------------------------------------------------------
 
 namespace {
