@@ -98,10 +98,10 @@ __device__ __forceinline__ int swz16(int r, int e) {
   return r * 16 + ((((e >> 1) ^ r) & 7) << 1) + (e & 1);
 }
 
-// DIRECT: operands come as 2-D TMA tiles of the caller's matrices (AK / BK:
+// DIRECT: operands come as 2-D TMA tiles of the caller's matrices (A_KC / B_KC:
 // k innermost, swizzled [128][16]; else m / n innermost, [16][128]); else
 // from PACK_FRAG64 panels by 1-D bulk copies.
-template <bool DIRECT, bool AK, bool BK>
+template <bool DIRECT, bool A_KC, bool B_KC>
 __global__ void __launch_bounds__(THREADS, 1)
     dmma_gemm_kernel(const __grid_constant__ DmmaGemmArgs p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -156,9 +156,9 @@ __global__ void __launch_bounds__(THREADS, 1)
             kl -= (int)p.kpair;
           }
           const int m0 = tm * BM, n0 = tn * BN;
-          if (AK) tc::tma_load_2d(dst, &p.ta[q], &full[stage], kl, m0);
+          if (A_KC) tc::tma_load_2d(dst, &p.ta[q], &full[stage], kl, m0);
           else tc::tma_load_2d(dst, &p.ta[q], &full[stage], m0, kl);
-          if (BK) tc::tma_load_2d(dst + TILE_BYTES, &p.tb[q], &full[stage], kl, n0);
+          if (B_KC) tc::tma_load_2d(dst + TILE_BYTES, &p.tb[q], &full[stage], kl, n0);
           else tc::tma_load_2d(dst + TILE_BYTES, &p.tb[q], &full[stage], n0, kl);
         } else {
           tc::bulk_load_1d(dst, ga + (long)kt * 4 * QUAD_DOUBLES, TILE_BYTES, &full[stage]);
@@ -209,13 +209,13 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int r = (wm * 4 + i) * 16 + g;
-            a0[i] = AK ? At[swz16(r, e)] : At[e * BM + r];
-            a1[i] = AK ? At[swz16(r + 8, e)] : At[e * BM + r + 8];
+            a0[i] = A_KC ? At[swz16(r, e)] : At[e * BM + r];
+            a1[i] = A_KC ? At[swz16(r + 8, e)] : At[e * BM + r + 8];
           }
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int c = (wn * 4 + j) * 8 + g;
-            b[j] = BK ? Bt[swz16(c, e)] : Bt[e * BN + c];
+            b[j] = B_KC ? Bt[swz16(c, e)] : Bt[e * BN + c];
           }
 #pragma unroll
           for (int i = 0; i < 4; ++i)
@@ -318,9 +318,9 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
-template <bool DIRECT, bool AK, bool BK>
+template <bool DIRECT, bool A_KC, bool B_KC>
 int launch_variant(const DmmaGemmArgs &a, int grid, cudaStream_t s) {
-  auto kern = dmma_gemm_kernel<DIRECT, AK, BK>;
+  auto kern = dmma_gemm_kernel<DIRECT, A_KC, B_KC>;
   static bool configured = false;
   if (!configured) {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
