@@ -398,6 +398,7 @@ FORM_CALLS = 10  # timed calls per form in the 8192 study (mean of one event pai
 def forms_study(torch, lib, n: int = 8192) -> dict:
     """Precision forms at m = n = k = n (8192 by default): one warm-up call,
     then FORM_CALLS back-to-back calls timed by one CUDA-event pair."""
+    import mublis_b200 as mb
     out = {}
     for p, dt, forms in (("s", torch.float32, ["plain", "bf16x3", "bf16x6", "fp16x3", "ozaki2"]),
                          ("d", torch.float64, ["plain", "ozaki:7", "ozaki:8", "ozaki2:14", "ozaki2"])):
@@ -406,6 +407,18 @@ def forms_study(torch, lib, n: int = 8192) -> dict:
         for i, x in enumerate((a, b, c)):
             fill(ctypes.c_void_p(x.data_ptr()), n, n, n, 0, i, 0)
         fn = getattr(lib, f"cblas_{p}gemm")
+        if p == "d":
+            # The modulus-count autotuner at two error targets: its choice
+            # (measured on the leading 256 x 256 block) and the form's speed.
+            for target in (1e-15, 1e-17):
+                nm, err = ctypes.c_int(), ctypes.c_double()
+                mb.check(lib.mublis_b200_ozaki2_autotune(
+                    b"d", 0, 0, n, n, n, ctypes.c_void_p(a.data_ptr()), 1, n,
+                    ctypes.c_void_p(b.data_ptr()), 1, n, target, ctypes.byref(nm),
+                    ctypes.byref(err)), lib)
+                out[f"dgemm_{n}_ozaki2@{target:g}_moduli"] = nm.value
+                out[f"dgemm_{n}_ozaki2@{target:g}_calibration_err"] = float(f"{err.value:.3g}")
+                forms = forms + [f"ozaki2@{target:g}"]
         for f in forms:
             lib.mublis_b200_set_form(p.encode(), f.encode())
             call = lambda: fn(COL, NT, NT, n, n, n, 1.0, ctypes.c_void_p(a.data_ptr()), n,  # noqa: E731
