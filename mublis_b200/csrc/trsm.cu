@@ -47,7 +47,16 @@ constexpr int LEAF = 64;  // diagonal blocks inverted by substitution
 // m * 512^2 extra flops).  With few right-hand sides that doubling step
 // would cost more than it saves, so 1024 is used only from m >= 4096 and
 // n >= 2048.
-int leaf_order(long m, long n) { return m >= 4096 && n >= 2048 ? 1024 : 512; }
+int leaf_order(long m, long n) {
+  // MUBLIS_B200_TRSM_LEAF=<256|512|1024> fixes it (tuning).
+  static const int forced = [] {
+    const char *e = getenv("MUBLIS_B200_TRSM_LEAF");
+    const int v = e ? atoi(e) : 0;
+    return v == 256 || v == 512 || v == 1024 ? v : 0;
+  }();
+  if (forced) return forced;
+  return m >= 4096 && n >= 2048 ? 1024 : 512;
+}
 
 // Leaves: FP64 solves use the fused leaf kernel (trsm_leaf.cu), FP32 solves
 // the inverted diagonal blocks applied as products; MUBLIS_B200_TRSM=fused /
