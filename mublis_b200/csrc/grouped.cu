@@ -41,13 +41,8 @@ struct GemmEntry {
 // ---- grouped GEMM kernel --------------------------------------------------------
 //
 // 256 threads as a 16 x 16 grid; each thread a TM x TN register tile, so a CTA
-// covers (16*TM) x (16*TN).  Operands stream into a 3-stage shared-memory
-// ring by element-wise cp.async with zero fill (bounds and any strides
-// handled by the copy, no registers held), two k-blocks ahead, and the
-// stream runs on across the CTA's consecutive tiles: the next tile's first
-// k-blocks load while the current one finishes and runs its epilogue
-// (with register-staged loads one block ahead, the loads' latency showed
-// as the main stall: long scoreboard, one CTA of 8 warps per SM).
+// covers (16*TM) x (16*TN).  Double-buffered shared memory with register
+// prefetch of the next k-block; loads follow whichever operand stride is 1.
 
 // Copies a run of V elements from shared memory (16- or 8-byte aligned when
 // the run is that long) into registers with one vector load.
@@ -65,31 +60,6 @@ __device__ __forceinline__ void lds_run(T *dst, const T *src) {
   }
 }
 
-// One element global -> shared, zero-filled when `valid` is false (the
-// source is then not read).
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T *dst, const T *src, bool valid) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  const int bytes = valid ? (int)sizeof(T) : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src),
-               "n"((int)sizeof(T)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_group() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-constexpr int GROUPED_STAGES = 3;
-
-template <typename T, int TM, int TN>
-constexpr int grouped_smem_bytes() {
-  return GROUPED_STAGES * (sizeof(T) == 8 ? 8 : 16) * 16 * (TM + TN) * (int)sizeof(T);
-}
-
 // `table` may be null: then the single problem `one` (passed by value in the
 // launch parameters) is the whole group -- the direct path for one small GEMM,
 // with no table upload.
@@ -99,10 +69,8 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
                                                            const __grid_constant__ GemmEntry one) {
   constexpr int BM = 16 * TM, BN = 16 * TN, BK = sizeof(T) == 8 ? 8 : 16;
   constexpr int A_PER = BM * BK / 256, B_PER = BK * BN / 256;
-  constexpr int STAGES = GROUPED_STAGES;
-  extern __shared__ __align__(16) unsigned char grouped_smem[];
-  T(*As)[BK][BM] = reinterpret_cast<T(*)[BK][BM]>(grouped_smem);
-  T(*Bs)[BK][BN] = reinterpret_cast<T(*)[BK][BN]>(grouped_smem + sizeof(T) * STAGES * BK * BM);
+  __shared__ __align__(16) T As[2][BK][BM];
+  __shared__ __align__(16) T Bs[2][BK][BN];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   // Thread (tx, ty) holds rows row0 + (i % VM) + 16 VM (i / VM) and columns
   // col0 + (j % VN) + 16 VN (j / VN): runs of up to 16 bytes, so each k step
@@ -114,60 +82,45 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
 
   // The table is followed by one int per output tile: the tile's problem.
   const int *tile_prob = table ? reinterpret_cast<const int *>(table + nprob) : nullptr;
-  auto entry = [&](int tile) -> const GemmEntry & { return table ? table[tile_prob[tile]] : one; };
-  auto kblocks_of = [&](const GemmEntry &e) { return (int)((e.k + BK - 1) / BK); };
+  for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    const GemmEntry &e = table ? table[tile_prob[tile]] : one;
+    const int local = tile - e.tile0;
+    const long m0 = (long)(local % e.tiles_m) * BM, n0 = (long)(local / e.tiles_m) * BN;
+    const T *A = (const T *)e.a, *B = (const T *)e.b;
+    const bool a_mfast = e.rs_a <= e.cs_a;  // i contiguous in memory
+    const bool b_kfast = e.rs_b <= e.cs_b;  // p contiguous in memory
 
-  // Issue cursor: the next (tile, k-block) to load, in this CTA's order of
-  // work; every issue is one commit group (empty past the last block), so
-  // group c is always k-block c of the stream.
-  int itile = blockIdx.x, ikb = 0;
-  auto advance = [&]() {  // skip to the next tile that has a k-block ikb
-    while (itile < total_tiles && ikb >= kblocks_of(entry(itile))) {
-      itile += gridDim.x;
-      ikb = 0;
-    }
-  };
-  long issued = 0;
-  auto issue = [&]() {
-    advance();
-    if (itile < total_tiles) {
-      const GemmEntry &e = entry(itile);
-      const int local = itile - e.tile0;
-      const long m0 = (long)(local % e.tiles_m) * BM, n0 = (long)(local / e.tiles_m) * BN;
-      const long k0 = (long)ikb * BK;
-      const T *A = (const T *)e.a, *B = (const T *)e.b;
-      const bool a_mfast = e.rs_a <= e.cs_a;  // i contiguous in memory
-      const bool b_kfast = e.rs_b <= e.cs_b;  // p contiguous in memory
-      const int slot = (int)(issued % STAGES);
+    T ra[A_PER], rb[B_PER];
+    auto gload = [&](long k0) {
 #pragma unroll
       for (int q = 0; q < A_PER; ++q) {
-        const int idx = tid + 256 * q;
-        const int i = a_mfast ? idx % BM : idx / BK, p = a_mfast ? idx / BM : idx % BK;
-        const long gi = m0 + i, gp = k0 + p;
-        const bool ok = gi < e.m && gp < e.k;
-        cp_async_elem(&As[slot][p][i], ok ? A + gi * e.rs_a + gp * e.cs_a : A, ok);
+        int idx = tid + 256 * q;
+        int i = a_mfast ? idx % BM : idx / BK, p = a_mfast ? idx / BM : idx % BK;
+        long gi = m0 + i, gp = k0 + p;
+        ra[q] = (gi < e.m && gp < e.k) ? A[gi * e.rs_a + gp * e.cs_a] : T(0);
       }
 #pragma unroll
       for (int q = 0; q < B_PER; ++q) {
-        const int idx = tid + 256 * q;
-        const int p = b_kfast ? idx % BK : idx / BN, j = b_kfast ? idx / BK : idx % BN;
-        const long gp = k0 + p, gj = n0 + j;
-        const bool ok = gp < e.k && gj < e.n;
-        cp_async_elem(&Bs[slot][p][j], ok ? B + gp * e.rs_b + gj * e.cs_b : B, ok);
+        int idx = tid + 256 * q;
+        int p = b_kfast ? idx % BK : idx / BN, j = b_kfast ? idx / BK : idx % BN;
+        long gp = k0 + p, gj = n0 + j;
+        rb[q] = (gp < e.k && gj < e.n) ? B[gp * e.rs_b + gj * e.cs_b] : T(0);
       }
-      ++ikb;
-    }
-    cp_async_commit_group();
-    ++issued;
-  };
+    };
+    auto sstore = [&](int buf) {
 #pragma unroll
-  for (int q = 0; q < STAGES - 1; ++q) issue();
-
-  long consumed = 0;
-  for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    const GemmEntry &e = entry(tile);
-    const int local = tile - e.tile0;
-    const long m0 = (long)(local % e.tiles_m) * BM, n0 = (long)(local / e.tiles_m) * BN;
+      for (int q = 0; q < A_PER; ++q) {
+        int idx = tid + 256 * q;
+        int i = a_mfast ? idx % BM : idx / BK, p = a_mfast ? idx / BM : idx % BK;
+        As[buf][p][i] = ra[q];
+      }
+#pragma unroll
+      for (int q = 0; q < B_PER; ++q) {
+        int idx = tid + 256 * q;
+        int p = b_kfast ? idx % BK : idx / BN, j = b_kfast ? idx / BK : idx % BN;
+        Bs[buf][p][j] = rb[q];
+      }
+    };
 
     // FP32 accumulates column pairs with the packed sm_100 FMA (__ffma2_rn:
     // two correctly rounded fmaf per instruction), halving the FMA issue
@@ -184,12 +137,16 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
         else acc[i][j] = T(0);
       }
 
-    const int kblocks = kblocks_of(e);
+    const int kblocks = (int)((e.k + BK - 1) / BK);
+    __syncthreads();  // previous tile's readers are done with the buffers
+    if (kblocks > 0) {
+      gload(0);
+      sstore(0);
+    }
+    __syncthreads();
     for (int kb = 0; kb < kblocks; ++kb) {
-      cp_async_wait_group<STAGES - 2>();  // this block's group has landed
-      __syncthreads();                    // ... for every thread; the slot
-      issue();                            // consumed last is free again
-      const int cur = (int)(consumed % STAGES);
+      const int cur = kb & 1;
+      if (kb + 1 < kblocks) gload((long)(kb + 1) * BK);
 #pragma unroll
       for (int p = 0; p < BK; ++p) {
         T af[TM], bf[TN];
@@ -208,7 +165,8 @@ __global__ void __launch_bounds__(256) grouped_gemm_kernel(const GemmEntry *__re
               acc[i][j] = fma(af[i], bf[j], acc[i][j]);
           }
       }
-      ++consumed;
+      if (kb + 1 < kblocks) sstore(cur ^ 1);
+      __syncthreads();
     }
 
     // Per row, the TN loads of C are issued before its stores (one memory
@@ -356,21 +314,11 @@ int launch_gemm_variant(int variant, const GemmEntry *dtable, int nprob, int til
   if (one) single = *one; else memset(&single, 0, sizeof single);
   B200ProfScope prof(one ? (sizeof(T) == 4 ? "direct_sgemm" : "direct_dgemm")
                          : (sizeof(T) == 4 ? "grouped_sgemm" : "grouped_dgemm"), s);
-  // Dynamic shared memory: the 3-stage ring (at most 48 KB, the 128 x 128
-  // classes; no opt-in needed, so this also works inside a graph capture).
   switch (variant) {
-  case TILE_32:
-    grouped_gemm_kernel<T, 2, 2><<<grid, 256, grouped_smem_bytes<T, 2, 2>(), s>>>(dtable, nprob, tiles, single);
-    break;
-  case TILE_64:
-    grouped_gemm_kernel<T, 4, 4><<<grid, 256, grouped_smem_bytes<T, 4, 4>(), s>>>(dtable, nprob, tiles, single);
-    break;
-  case TILE_128x64:
-    grouped_gemm_kernel<T, 8, 4><<<grid, 256, grouped_smem_bytes<T, 8, 4>(), s>>>(dtable, nprob, tiles, single);
-    break;
-  default:
-    grouped_gemm_kernel<T, 8, 8><<<grid, 256, grouped_smem_bytes<T, 8, 8>(), s>>>(dtable, nprob, tiles, single);
-    break;
+  case TILE_32: grouped_gemm_kernel<T, 2, 2><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  case TILE_64: grouped_gemm_kernel<T, 4, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  case TILE_128x64: grouped_gemm_kernel<T, 8, 4><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
+  default: grouped_gemm_kernel<T, 8, 8><<<grid, 256, 0, s>>>(dtable, nprob, tiles, single); break;
   }
   B200_LAUNCH_CHECK();
   return B200_OK;
