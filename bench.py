@@ -512,18 +512,21 @@ def _grouped_sgemms(torch, rng):
     return probs, keep, (mb.GemmProblem * len(probs))(*probs)
 
 
-def grouped_direct(torch, lib) -> dict:
-    """Config 4's SGEMMs as direct grouped calls (no plan, no autotuning): one
-    warm-up call, then five timed, three kernel launches per call (one per
-    tile class).  For profiler captures of the grouped kernel."""
+def grouped_direct(torch, lib, form: str = "plain") -> dict:
+    """Config 4's SGEMMs as direct grouped calls (no plan, no autotuning) in
+    the given FP32 form: one warm-up call, then five timed (plain: three
+    kernel launches per call, one per tile class; fp16x3: a pack and one
+    tensor-core launch).  For profiler captures of the grouped kernels."""
     import numpy as np
     import mublis_b200 as mb
     probs, keep, arr = _grouped_sgemms(torch, np.random.default_rng(1))
     gflop = sum(2.0 * p.m * p.n * p.k for p in probs)
+    mb.check(lib.mublis_b200_set_form(b"s", form.encode()), lib)
     mb.check(lib.mublis_b200_gemm_grouped(b"s", arr, len(probs)), lib)
     ms = timed(torch, lambda: lib.mublis_b200_gemm_grouped(b"s", arr, len(probs)), 5)
+    lib.mublis_b200_set_form(b"s", b"plain")
     del keep
-    return {"gflop": round(gflop / 1e9, 2), "ms": round(ms, 3),
+    return {"form": form, "gflop": round(gflop / 1e9, 2), "ms": round(ms, 3),
             "tflops": round(gflop / ms / 1e9, 2)}
 
 
@@ -542,6 +545,13 @@ def grouped_study(torch, lib) -> dict:
     plan = ctypes.c_void_p()
     mb.check(lib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)), lib)
     ms_plan = timed(torch, lambda: lib.mublis_b200_plan_run(plan), 10)
+    lib.mublis_b200_plan_destroy(plan)
+    # The same group on the tensor cores (FP32 form fp16x3: tc_grouped.cu).
+    lib.mublis_b200_set_form(b"s", b"fp16x3")
+    plan = ctypes.c_void_p()
+    mb.check(lib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)), lib)
+    ms_tc = timed(torch, lambda: lib.mublis_b200_plan_run(plan), 10)
+    lib.mublis_b200_set_form(b"s", b"plain")
 
     def loop():
         for p in probs:
@@ -576,6 +586,8 @@ def grouped_study(torch, lib) -> dict:
     torch.cuda.empty_cache()
     return {"sgemm_x4096": {"gflop": round(gflop / 1e9, 2), "grouped_ms": round(ms_plan, 3),
                             "grouped_tflops": round(gflop / ms_plan / 1e9, 2),
+                            "grouped_fp16x3_ms": round(ms_tc, 3),
+                            "grouped_fp16x3_tflops": round(gflop / ms_tc / 1e9, 2),
                             "one_call_per_launch_ms": round(ms_loop, 2),
                             "speedup": round(ms_loop / ms_plan, 1)},
             "dtrsm_x1024": {"gflop": round(tflop / 1e9, 3), "grouped_ms": round(ms_tplan, 3),
@@ -777,6 +789,8 @@ def main():
                     help="run only the TRSM/TRMM side x uplo x transpose study")
     ap.add_argument("--only-grouped", action="store_true",
                     help="run only config 4's SGEMMs as direct grouped calls (profiler captures)")
+    ap.add_argument("--grouped-form", default="plain", choices=["plain", "fp16x3"],
+                    help="FP32 form of --only-grouped")
     ap.add_argument("--only-trsm", default=None, choices=["s", "d"],
                     help="run only two TRSMs of order --n with --n right-hand sides "
                          "(left, lower, non-unit; profiler captures of the TRSM kernels)")
@@ -833,7 +847,7 @@ def main():
 
     if args.only_grouped:
         if rank == 0:
-            print(json.dumps({"grouped_direct": grouped_direct(torch, lib)}))
+            print(json.dumps({"grouped_direct": grouped_direct(torch, lib, args.grouped_form)}))
         return
 
     if args.only_forms:

@@ -674,6 +674,7 @@ struct mublis_b200_plan {
   int kind = 0;  // 0 gemm, 1 trsm
   GemmGroup gg[NCLASS];
   TrsmGroup tg;
+  b200_tcg *tcg = nullptr;  // FP32 GEMMs in the fp16x3 form
   std::vector<mublis_b200_trsm_problem_t> trsm_problems;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -705,12 +706,20 @@ int plan_gemm(mublis_b200_plan *pl, const mublis_b200_gemm_problem_t *p, int cou
   return st;
 }
 
+// FP32 groups run in the fp16x3 tensor-core form (tc_grouped.cu) when that
+// is the FP32 form; every other form runs the plain grouped kernel.
+bool tc_grouped(char dtype) {
+  return dtype == 's' && b200_get_default_form(B200_F32) == B200_FORM_FP16X3;
+}
+
 int capture(mublis_b200_plan *pl) {
   cudaStream_t s = b200_cur_stream();
   B200_TRY(b200_stream_sync());
   B200_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int st;
-  if (pl->kind == 0)
+  if (pl->tcg)
+    st = b200_tcg_run(pl->tcg, s);
+  else if (pl->kind == 0)
     st = pl->dtype == 'd' ? run_groups<double>(pl->gg, s) : run_groups<float>(pl->gg, s);
   else
     st = pl->dtype == 'd' ? launch_trsm_group<double>(pl->tg, s) : launch_trsm_group<float>(pl->tg, s);
@@ -887,6 +896,14 @@ int mublis_b200_gemm_grouped(char dtype, const mublis_b200_gemm_problem_t *probl
   if (count == 0) return B200_OK;
   B200_TRY(b200_init());
   cudaStream_t s = b200_cur_stream();
+  if (tc_grouped(dtype)) {
+    b200_tcg *g = nullptr;
+    B200_TRY(b200_tcg_create(problems, count, &g));
+    int st = b200_tcg_run(g, s);
+    if (st == B200_OK) st = b200_stream_sync();
+    b200_tcg_destroy(g);
+    return st == B200_OK ? b200_stream_sync() : st;
+  }
   std::vector<GemmEntry> cls[NCLASS];
   B200_TRY(to_entries(dtype, problems, count, cls));
   GemmGroup g[NCLASS];
@@ -931,7 +948,9 @@ int mublis_b200_plan_gemm_grouped(char dtype, const mublis_b200_gemm_problem_t *
   auto *pl = new mublis_b200_plan;
   pl->dtype = dtype;
   pl->kind = 0;
-  int st = dtype == 'd' ? plan_gemm<double>(pl, problems, count) : plan_gemm<float>(pl, problems, count);
+  int st = tc_grouped(dtype) ? b200_tcg_create(problems, count, &pl->tcg)
+           : dtype == 'd'    ? plan_gemm<double>(pl, problems, count)
+                             : plan_gemm<float>(pl, problems, count);
   if (st == B200_OK) st = capture(pl);
   if (st != B200_OK) {
     mublis_b200_plan_destroy(pl);
@@ -978,6 +997,7 @@ int mublis_b200_plan_destroy(mublis_b200_plan_t *plan) {
   if (plan->graph) cudaGraphDestroy(plan->graph);
   for (auto &g : plan->gg) b200_free(g.dtable);
   b200_free(plan->tg.dtable);
+  b200_tcg_destroy(plan->tcg);
   b200_stream_sync();
   delete plan;
   return B200_OK;

@@ -7,6 +7,17 @@
 int tc_run_bf16(const b200_l3_desc_t *d, int form);
 int tc_run_ozaki(const b200_l3_desc_t *d);
 
+#include "../../include/mublis_b200.h"
+
+// tc_grouped.cu: a group of FP32 GEMMs in the fp16x3 form.  create builds
+// the device tables and staging areas (synchronous; not during capture),
+// run launches the pack and the tensor-core kernel on `s` (capturable),
+// destroy frees them.
+struct b200_tcg;
+int b200_tcg_create(const mublis_b200_gemm_problem_t *p, int count, b200_tcg **out);
+int b200_tcg_run(b200_tcg *g, cudaStream_t s);
+void b200_tcg_destroy(b200_tcg *g);
+
 #include <string>
 
 // ozaki_tune.cu: the modulus count of the modular form for a target

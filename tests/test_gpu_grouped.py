@@ -213,3 +213,109 @@ def test_tuned_table_round_trip(glib, tmp_path):
     missing = tmp_path / "missing.txt"
     assert glib.mublis_b200_tune_load(str(missing).encode(), ctypes.byref(entries)) == 0
     assert entries.value == 0
+
+
+@pytest.fixture
+def fp16x3(glib):
+    glib.mublis_b200_set_form(b"s", b"fp16x3")
+    yield glib
+    glib.mublis_b200_set_form(b"s", b"plain")
+
+
+def _edge_gemms(torch):
+    """Problems at the edges of the tensor-core grouped path: 1 x 1 x 1,
+    k = 0 and alpha = 0 (beta * C only), beta = 0 over a NaN C, rows and
+    columns far apart in magnitude (per-row / per-column scaling), ragged
+    sizes on both sides of 128 and of the 16 / 32 / 64 column widths, and
+    k past one 512-k pack strip."""
+    out = []
+    for (m, n, k, al, be) in [(1, 1, 1, 1.0, 0.5), (130, 17, 0, 1.0, 0.5), (40, 33, 50, 0.0, 2.0),
+                              (129, 65, 300, 1.25, 0.0), (257, 129, 513, 0.75, 0.25),
+                              (16, 16, 16, 1.0, 1.0), (8, 200, 31, 1.0, -0.5),
+                              (70, 90, 1100, 0.5, 0.5)]:
+        a = torch.rand(max(k, 1), m, device="cuda") * 2 - 1
+        b = torch.rand(n, max(k, 1), device="cuda") * 2 - 1
+        c = torch.rand(n, m, device="cuda") * 2 - 1
+        if be == 0.0:
+            c.fill_(float("nan"))
+        if m == 129:  # op(A) row 3 and op(B) column 5 far from the others
+            a[:, 3] *= 2.0 ** 40
+            b[5, :] *= 2.0 ** -40
+        out.append((GemmProblem(0, 0, m, n, k, al, be, a.data_ptr(), m, b.data_ptr(), max(k, 1),
+                                c.data_ptr(), m), (a, b, c)))
+    return out
+
+
+def test_grouped_fp16x3_equals_single_fp16x3_calls(fp16x3):
+    """With the FP32 form fp16x3 a group runs on the tensor cores
+    (tc_grouped.cu) and gives, problem by problem, the bits of single
+    fp16x3 calls (same scaling, split, product order and 256-k windows);
+    both stay within 4 k u of plain FP32 calls."""
+    torch = pytest.importorskip("torch")
+    glib = fp16x3
+    probs, keep = make_gemm_set(torch, "s", 96, seed=11, hi=700)
+    for pr, k3 in _edge_gemms(torch):
+        probs.append(pr)
+        keep.append(k3)
+    c0 = [c.clone() for _, _, c in keep]
+    arr = (GemmProblem * len(probs))(*probs)
+    n0 = glib.mublis_b200_launch_count()
+    assert glib.mublis_b200_gemm_grouped(b"s", arr, len(probs)) == 0, mb.last_error(glib)
+    assert glib.mublis_b200_launch_count() - n0 == 2  # pack + one persistent launch
+    grouped = [c.clone() for _, _, c in keep]
+    for q, pr in enumerate(probs):
+        assert not grouped[q].isnan().any(), (q, pr.m, pr.n, pr.k)
+        keep[q][2].copy_(c0[q])
+        assert single_call(glib, "s", pr) == 0
+        assert torch.equal(grouped[q], keep[q][2]), (q, pr.m, pr.n, pr.k)
+    glib.mublis_b200_set_form(b"s", b"plain")
+    for q, pr in enumerate(probs):
+        keep[q][2].copy_(c0[q])
+        assert single_call(glib, "s", pr) == 0
+        a, b, _ = keep[q]
+        c0n = c0[q].nan_to_num().norm().item() if pr.beta != 0 else 0.0
+        den = abs(pr.alpha) * a.norm().item() * b.norm().item() + abs(pr.beta) * c0n
+        err = (grouped[q].double() - keep[q][2].double()).norm().item() / max(den, 1e-300)
+        assert err <= 4 * max(pr.k, 1) * 2.0 ** -24, (q, pr.m, pr.n, pr.k, err)
+
+
+def test_grouped_fp16x3_against_oracle(fp16x3):
+    torch = pytest.importorskip("torch")
+    glib = fp16x3
+    m, n, k = 200, 77, 333
+    a = orc.fill(k, m, np.float32, 6, 0)   # op(A) = A^T
+    b = orc.fill(n, k, np.float32, 6, 1)   # op(B) = B^T
+    c0 = orc.fill(m, n, np.float32, 6, 2)
+    ta, tb, tc = (torch.from_numpy(x.T.copy()).cuda() for x in (a, b, c0))
+    pr = GemmProblem(1, 1, m, n, k, 0.75, 0.25, ta.data_ptr(), k, tb.data_ptr(), n,
+                     tc.data_ptr(), m)
+    assert glib.mublis_b200_gemm_grouped(b"s", (GemmProblem * 1)(pr), 1) == 0
+    ref = c0.copy(order="F")
+    assert orc.restated().oracle_sgemm(1, 1, m, n, k, 0.75, a.ctypes.data, 1, k, b.ctypes.data,
+                                       1, n, 0.25, ref.ctypes.data, 1, m) == 0
+    got = tc.cpu().numpy().T
+    err = np.linalg.norm(got - ref) / (0.75 * np.linalg.norm(a) * np.linalg.norm(b) +
+                                       0.25 * np.linalg.norm(c0))
+    assert err <= 4 * k * 2.0 ** -24
+
+
+def test_grouped_fp16x3_plan_replay(fp16x3):
+    """A plan in the fp16x3 form captures the two launches; creating it runs
+    nothing (C unchanged) and its replay equals a direct grouped call."""
+    torch = pytest.importorskip("torch")
+    glib = fp16x3
+    probs, keep = make_gemm_set(torch, "s", 64, seed=13)
+    c0 = [c.clone() for _, _, c in keep]
+    arr = (GemmProblem * len(probs))(*probs)
+    plan = ctypes.c_void_p()
+    assert glib.mublis_b200_plan_gemm_grouped(b"s", arr, len(probs), ctypes.byref(plan)) == 0
+    for q in range(len(probs)):
+        assert torch.equal(keep[q][2], c0[q])
+    assert glib.mublis_b200_plan_run(plan) == 0
+    replay = [c.clone() for _, _, c in keep]
+    for q in range(len(probs)):
+        keep[q][2].copy_(c0[q])
+    assert glib.mublis_b200_gemm_grouped(b"s", arr, len(probs)) == 0
+    for q in range(len(probs)):
+        assert torch.equal(replay[q], keep[q][2])
+    assert glib.mublis_b200_plan_destroy(plan) == 0
