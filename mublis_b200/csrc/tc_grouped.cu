@@ -57,6 +57,7 @@ constexpr int TCG_SMEM = TCG_STAGES * TCG_STAGE_BYTES + 1024 + 256;
 constexpr int TCG_PRODUCER_REGS = 56, TCG_EPILOGUE_REGS = 216;
 constexpr int TCG_PACK_NBUF = 3;    // strips in the pack ring: two in flight while one is split
 constexpr int TCG_PACK_KS = 512;    // k a strip buffer holds; longer rows are read twice
+constexpr int TCG_PACK_WARPS = 8;   // warps per pack CTA
 
 // Pack-side view of one problem.
 struct TcgProblem {
@@ -109,10 +110,15 @@ __device__ __forceinline__ void tcg_scale_factors(int e, float &f1, float &f2) {
   f2 = __int_as_float((sh - s1 + 127) << 23);
 }
 
-__device__ __forceinline__ void tcg_split(float x, float f1, float f2, __half &h, __half &l) {
-  const float xs = (x * f1) * f2;
-  h = __float2half_rn(xs);
-  l = __float2half_rn(xs - __half2float(h));
+// The scale exponent of b200_scale_exp (frexp's: max|x| < 2^e, 0 for an
+// all-zero row) from the bits of a non-negative float, by integer
+// arithmetic: normal E - 126, subnormal -117 - clz(mantissa); infinity and
+// NaN take b200_scale_exp itself.
+__device__ __forceinline__ int tcg_exp_of(unsigned bits) {
+  const int E = (int)(bits >> 23);
+  if (E == 0) return bits == 0 ? 0 : -117 - __clz((int)bits);
+  if (E < 255) return E - 126;
+  return b200_scale_exp((unsigned long long)__double_as_longlong((double)__uint_as_float(bits)));
 }
 
 // 4-byte asynchronous copy global -> shared (zero-filled when !valid; src
@@ -158,33 +164,35 @@ __device__ __forceinline__ TcgStrip tcg_strip(const TcgProblem *probs, const Tcg
 template <bool ASYNC>
 __device__ __forceinline__ void tcg_fill(const TcgStrip &v, float *buf, int ld, int k0, int w) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kin = max(0, min(w, v.k - k0));  // strip columns [0, kin) exist in the matrix
+  auto put = [&](float *dst, const float *src) {
+    if (ASYNC)
+      tcg_cp4(dst, src, true);
+    else
+      *dst = *src;
+  };
   if (v.rs == 1 || v.kst != 1) {
     const long gr = (long)v.row0 + lane;
-    const bool rin = gr < v.rows;
-    const float *xr = v.x + (rin ? gr * v.rs : 0);
+    float *d = buf + lane * ld;
+    int kk = warp;
+    if (gr < v.rows) {
+      const float *src = v.x + gr * v.rs + ((long)k0 + warp) * v.kst;
+      const long step = TCG_PACK_WARPS * v.kst;
 #pragma unroll 4
-    for (int kk = warp; kk < w; kk += 8) {
-      const long gk = (long)k0 + kk;
-      const bool ok = rin && gk < v.k;
-      if (ASYNC)
-        tcg_cp4(&buf[lane * ld + kk], ok ? xr + gk * v.kst : v.x, ok);
-      else
-        buf[lane * ld + kk] = ok ? xr[gk * v.kst] : 0.f;
+      for (; kk < kin; kk += TCG_PACK_WARPS, src += step) put(d + kk, src);
     }
+    for (; kk < w; kk += TCG_PACK_WARPS) d[kk] = 0.f;  // past k, or past the matrix's rows
   } else {
-    for (int r = warp; r < 32; r += 8) {
+    for (int r = warp; r < 32; r += TCG_PACK_WARPS) {
       const long gr = (long)v.row0 + r;
-      const bool rin = gr < v.rows;
-      const float *xr = v.x + (rin ? gr * v.rs : 0);
+      float *d = buf + r * ld;
+      int kk = lane;
+      if (gr < v.rows) {
+        const float *src = v.x + gr * v.rs + k0 + lane;
 #pragma unroll 4
-      for (int kk = lane; kk < w; kk += 32) {
-        const long gk = (long)k0 + kk;
-        const bool ok = rin && gk < v.k;
-        if (ASYNC)
-          tcg_cp4(&buf[r * ld + kk], ok ? xr + gk : v.x, ok);
-        else
-          buf[r * ld + kk] = ok ? xr[gk] : 0.f;
+        for (; kk < kin; kk += 32, src += 32) put(d + kk, src);
       }
+      for (; kk < w; kk += 32) d[kk] = 0.f;
     }
   }
 }
@@ -194,32 +202,44 @@ __device__ __forceinline__ void tcg_fill(const TcgStrip &v, float *buf, int ld, 
 // their k; strips of up to 512 k go through a ring of three shared-memory
 // buffers filled by cp.async two strips ahead; longer ones are read twice
 // in 512-k chunks (abs-max, then split).
-__global__ void __launch_bounds__(256, 1) tcg_pack_kernel(const TcgProblem *__restrict__ probs,
+__global__ void __launch_bounds__(TCG_PACK_WARPS * 32, 1) tcg_pack_kernel(const TcgProblem *__restrict__ probs,
                                                           const TcgPackTask *__restrict__ tasks,
                                                           int ntasks, int ks,
                                                           unsigned char *__restrict__ stage_a,
                                                           unsigned char *__restrict__ stage_b,
                                                           int *__restrict__ exps) {
   extern __shared__ float ring[];  // TCG_PACK_NBUF x 32 x (ks + 1)
-  __shared__ float part[8][32];
-  __shared__ int rexp[32];
+  __shared__ unsigned rmax[32];  // bits of each strip row's abs-max (non-negative floats order as ints)
   const int ld = ks + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int mine = ntasks > (int)blockIdx.x ? (ntasks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   auto buf_of = [&](int i) { return ring + (i % TCG_PACK_NBUF) * 32 * ld; };
-  auto task_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
-  auto issue = [&](int i) {  // start strip i's copies (strips that fit a buffer only)
-    if (i < mine) {
-      const TcgStrip v = tcg_strip(probs, tasks, task_of(i));
-      if (v.kb * TCG_BK <= ks) tcg_fill<true>(v, buf_of(i), ld, 0, v.kb * TCG_BK);
-    }
+  // Strip descriptors run three ahead in registers, so the dependent loads
+  // (task, then problem) of a strip overlap the work on earlier ones.
+  auto view = [&](int i) {
+    TcgStrip v;
+    if (i < mine) return tcg_strip(probs, tasks, (int)blockIdx.x + i * (int)gridDim.x);
+    memset(&v, 0, sizeof v);
+    return v;
+  };
+  auto issue = [&](const TcgStrip &v, int i) {  // start strip i's copies (strips that fit a buffer)
+    if (i < mine && v.kb * TCG_BK <= ks) tcg_fill<true>(v, buf_of(i), ld, 0, v.kb * TCG_BK);
     tcg_cp_commit();
   };
-  for (int i = 0; i < TCG_PACK_NBUF - 1; ++i) issue(i);
+  if (threadIdx.x < 32) rmax[threadIdx.x] = 0u;
+  static_assert(TCG_PACK_NBUF == 3, "the descriptor rotation below assumes a ring of three");
+  TcgStrip v0 = view(0), v1 = view(1);
+  issue(v0, 0);
+  issue(v1, 1);
+  TcgStrip v2 = view(2);
 
   for (int i = 0; i < mine; ++i) {
-    issue(i + TCG_PACK_NBUF - 1);
-    const TcgStrip v = tcg_strip(probs, tasks, task_of(i));
+    issue(v2, i + 2);
+    const TcgStrip v3 = view(i + 3);
+    const TcgStrip v = v0;
+    v0 = v1;
+    v1 = v2;
+    v2 = v3;
     float *buf = buf_of(i);
     const int kb = v.kb, kpad = kb * TCG_BK;
     const bool resident = kpad <= ks;
@@ -227,7 +247,9 @@ __global__ void __launch_bounds__(256, 1) tcg_pack_kernel(const TcgProblem *__re
       tcg_cp_wait<TCG_PACK_NBUF - 1>();  // this strip's group has landed
       __syncthreads();
     }
-    // Abs-max of each row over k (lane = row, warp = k residue mod 8).
+    // Abs-max of each row over k (lane = row, warp = k residue), folded into
+    // rmax by shared-memory atomics (cleared at the end of the previous
+    // strip).
     float mx = 0.f;
     for (int k0 = 0; k0 < kpad; k0 += ks) {
       const int w = min(ks, kpad - k0);
@@ -236,18 +258,12 @@ __global__ void __launch_bounds__(256, 1) tcg_pack_kernel(const TcgProblem *__re
         tcg_fill<false>(v, buf, ld, k0, w);
         __syncthreads();
       }
-      for (int kk = warp; kk < w; kk += 8) mx = fmaxf(mx, fabsf(buf[lane * ld + kk]));
+      for (int kk = warp; kk < w; kk += TCG_PACK_WARPS) mx = fmaxf(mx, fabsf(buf[lane * ld + kk]));
     }
-    part[warp][lane] = mx;
+    atomicMax(&rmax[lane], __float_as_uint(mx));
     __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-      for (int q = 1; q < 8; ++q) mx = fmaxf(mx, part[q][lane]);
-      const int e = b200_scale_exp((unsigned long long)__double_as_longlong((double)mx));
-      rexp[lane] = e;
-      if (v.row0 + lane < v.rows) exps[(v.side ? v.p->eb : v.p->ea) + v.row0 + lane] = e;
-    }
-    __syncthreads();
+    if (threadIdx.x < 32 && v.row0 + lane < v.rows)
+      exps[(v.side ? v.p->eb : v.p->ea) + v.row0 + lane] = tcg_exp_of(rmax[lane]);
     // Split and store: item (k-block, row, 16-byte chunk), four consecutive
     // lanes writing one row's 64 bytes.
     const int blk = v.row0 / TCG_BM, r0 = v.row0 % TCG_BM;  // the strip lies in one 128-row block
@@ -262,15 +278,20 @@ __global__ void __launch_bounds__(256, 1) tcg_pack_kernel(const TcgProblem *__re
         __syncthreads();
       }
       const int items = (w / TCG_BK) * 128;
-      for (int it = threadIdx.x; it < items; it += 256) {
+      for (int it = threadIdx.x; it < items; it += TCG_PACK_WARPS * 32) {
         const int ch = it & 3, r = (it >> 2) & 31, cl = it >> 7;
         if (r >= nr) continue;
         float f1, f2;
-        tcg_scale_factors(rexp[r], f1, f2);
+        tcg_scale_factors(tcg_exp_of(rmax[r]), f1, f2);
         const float *src = buf + r * ld + cl * TCG_BK + ch * 8;
-        __align__(16) __half h[8], l[8];
+        __align__(16) __half2 h[4], l[4];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) tcg_split(src[j], f1, f2, h[j], l[j]);
+        for (int j = 0; j < 4; ++j) {  // two elements per conversion
+          const float a = (src[2 * j] * f1) * f2, b = (src[2 * j + 1] * f1) * f2;
+          h[j] = __floats2half2_rn(a, b);
+          const float2 hf = __half22float2(h[j]);
+          l[j] = __floats2half2_rn(a - hf.x, b - hf.y);
+        }
         unsigned char *dst =
             tiles0 + ((long)(k0 / TCG_BK + cl) * 2) * TCG_TILE + tcg_swz(r0 + r, ch);
         *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(h);
@@ -278,6 +299,7 @@ __global__ void __launch_bounds__(256, 1) tcg_pack_kernel(const TcgProblem *__re
       }
     }
     __syncthreads();  // the buffer is free for the strip issued next iteration
+    if (threadIdx.x < 32) rmax[threadIdx.x] = 0u;  // read by no one until the next barrier
   }
   tcg_cp_wait<0>();
 }
@@ -710,7 +732,7 @@ int b200_tcg_run(b200_tcg *g, cudaStream_t s) {
     const size_t smem = sizeof(float) * TCG_PACK_NBUF * 32 * (ks + 1);
     const int grid = std::min(g->ntasks, b200_sm_count());
     B200ProfScope prof("tcg_pack", s);
-    tcg_pack_kernel<<<grid, 256, smem, s>>>(g->probs, g->tasks, g->ntasks, ks, g->stage_a,
+    tcg_pack_kernel<<<grid, TCG_PACK_WARPS * 32, smem, s>>>(g->probs, g->tasks, g->ntasks, ks, g->stage_a,
                                             g->stage_b, g->exps);
     B200_LAUNCH_CHECK();
   }
