@@ -430,6 +430,317 @@ __global__ void __launch_bounds__(384, 1)
   }
 }
 
+// ---- CTA-pair form ----------------------------------------------------------
+//
+// The same contraction with 256 x 256 tiles on a pair of SMs (a cluster of
+// two CTAs, tcgen05 cta_group::2).  Each CTA TMA-loads its 128 rows of
+// op(A) and its 128 rows (columns of the tile) of op(B) into its own shared
+// memory, completing the bytes on the leader's (rank 0) stage barrier; the
+// leader issues the M = 256, N = 256 MMAs, which read both CTAs' tiles and
+// write each CTA's 128 accumulator rows into that CTA's TMEM; its commits
+// arrive on the stage-free and window-ready barriers of both CTAs; each
+// epilogue warp releases a window on the leader's barrier.  Per SM and MMA
+// the tensor cores read 4 KB of A and 4 KB of B from shared memory instead
+// of 4 KB and 8 KB, which is what bounds the three-product forms on one SM
+// (operand reads plus the TMA fills exceed the shared-memory bandwidth).
+// The MMA sequence per output element (k order, products, windows) is the
+// single-SM kernel's.
+template <int TERMS, int STAGES>
+struct Bf16PairCfg {
+  static constexpr int BM = 128, BN = 128, SWZ = 64, BK = SWZ / 2;  // per CTA
+  static constexpr int TILE_M = 256, TILE_N = 256;                  // per pair
+  static constexpr int A_TILE = BM * SWZ, B_TILE = BN * SWZ;
+  static constexpr int STAGE_BYTES = TERMS * (A_TILE + B_TILE);
+  static constexpr int KSTEPS = SWZ / 32;
+  static constexpr int FLUSH = 8;
+  static constexpr int THREADS = 384;
+  static constexpr int EPI_WARPS = 8;
+  static constexpr int HALF = TILE_N / 2;  // columns per epilogue thread
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr uint32_t TMEM_COLS = 512;
+};
+
+template <int TERMS, int STAGES, bool F16 = false>
+__global__ void __launch_bounds__(384, 1)
+    tc_bf16_pair_kernel(const __grid_constant__ CUtensorMap tmA,
+                        const __grid_constant__ CUtensorMap tmB, Bf16Params p) {
+  using C = Bf16PairCfg<TERMS, STAGES>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = tc::cluster_rank();
+  const bool leader = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);   // leader: its expect_tx; bytes of both CTAs
+      tc::mbar_init(&empty[s], 1);  // the leader's commit, in both CTAs
+    }
+    for (int a = 0; a < 2; ++a) {
+      tc::mbar_init(&tfull[a], 1);
+      tc::mbar_init(&tempty[a], 2 * C::EPI_WARPS);  // leader: one arrival per epilogue warp of the pair
+    }
+    tc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    tc::fence_barrier_init();
+    tc::tma_prefetch_desc(&tmA);
+    tc::tma_prefetch_desc(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc_pair(tmem_slot, C::TMEM_COLS);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();  // both CTAs' barriers initialised before any remote use
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const TileWalk &w = p.w;  // bm = bn = 256: pair tiles
+  const int num_tiles = w.tiles_m * w.tiles_n;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  auto sa = [&](int s, int t) { return smem + s * C::STAGE_BYTES + t * C::A_TILE; };
+  auto sb = [&](int s, int t) {
+    return smem + s * C::STAGE_BYTES + TERMS * C::A_TILE + t * C::B_TILE;
+  };
+
+  if (warp < 4) {
+  tc::setmaxnreg_dec<TC_PRODUCER_REGS>();
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    int stage = 0;
+    uint32_t phase = 0;
+    int issued = 0;
+    bool ok = true;
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const int arow = (int)((long)tm * C::TILE_M + rank * C::BM);
+      const int brow = (int)((long)tn * C::TILE_N + rank * C::BN);
+      for (int kb = kb0; kb < kb1; ++kb) {
+        if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        if (leader) tc::mbar_arrive_expect_tx(&full[stage], 2 * C::STAGE_BYTES);
+        const uint32_t fb = tc::map_rank(&full[stage], 0);
+#pragma unroll
+        for (int t = 0; t < TERMS; ++t)
+          tc::tma_load_2d_pair(sa(stage, t), &tmA, fb, kb * C::BK, (int)(t * p.mpad + arow));
+#pragma unroll
+        for (int t = 0; t < TERMS; ++t)
+          tc::tma_load_2d_pair(sb(stage, t), &tmB, fb, kb * C::BK, (int)(t * p.npad + brow));
+        ++issued;
+        if (++stage == STAGES) { stage = 0; phase ^= 1; }
+      }
+    }
+    // Drain (leader): the last ring's worth of stages has landed in both
+    // CTAs (their bytes complete on the leader's barriers).
+    if (leader) {
+      int pending = issued < STAGES ? issued : STAGES;
+      for (int q = 0; q < pending; ++q) {
+        if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
+        if (!tc::mbar_wait_drain(&full[stage], phase)) break;
+      }
+    }
+  } else if (warp == 1 && lane == 0 && leader) {
+    // ---------------- MMA issuer (leader) ----------------
+    constexpr uint32_t IDESC = F16 ? tc::idesc_f16(C::TILE_M, C::TILE_N)
+                                   : tc::idesc_bf16(C::TILE_M, C::TILE_N);
+    int stage = 0, acc = 0;
+    uint32_t phase = 0, acc_phase = 0;
+    bool ok = true, any = false;
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += C::FLUSH) {
+        const int c1 = min(kb1, c0 + C::FLUSH);
+        // Both CTAs' epilogues have drained this window buffer.
+        if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+        tc::tc_fence_after();
+        const uint32_t d = tmem_base + (uint32_t)(acc * C::TILE_N);
+        for (int kb = c0; kb < c1; ++kb) {
+          if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
+          tc::tc_fence_after();
+#pragma unroll
+          for (int ks = 0; ks < C::KSTEPS; ++ks) {
+#pragma unroll
+            for (int sum = TERMS - 1; sum >= 0; --sum) {
+#pragma unroll
+              for (int ta = 0; ta <= sum; ++ta) {
+                const int tb = sum - ta;
+                uint64_t ad = tc::smem_desc(sa(stage, ta), C::SWZ) + (uint64_t)((ks * 32) >> 4);
+                uint64_t bd = tc::smem_desc(sb(stage, tb), C::SWZ) + (uint64_t)((ks * 32) >> 4);
+                const bool first = kb == c0 && ks == 0 && sum == TERMS - 1 && ta == 0;
+                tc::mma_f16_pair(d, ad, bd, IDESC, first ? 0u : 1u);
+              }
+            }
+          }
+          tc::mma_commit_pair(&empty[stage]);
+          any = true;
+          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+        tc::mma_commit_pair(&tfull[acc]);
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+      }
+    }
+    if (any) {  // every issued MMA has completed before TMEM is released
+      tc::mma_commit_pair(drain);
+      tc::mbar_wait(drain, 0, abort_flag, p.err);
+    }
+  }
+  } else {
+    tc::setmaxnreg_inc<TC_EPILOGUE_REGS>();
+    // ---------------- epilogue (both CTAs: this CTA's 128 rows) ----------------
+    const int quad = warp & 3;
+    const int half = (warp - 4) >> 2;
+    const int row = quad * 32 + lane;
+    const uint32_t lane_base = tmem_base + ((uint32_t)(quad * 32) << 16);
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    float run[C::HALF];
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const long gi = (long)tm * C::TILE_M + rank * C::BM + row;
+      const bool row_ok = gi < w.m;
+      const long gj0 = (long)tn * C::TILE_N + half * C::HALF;
+      if (kb0 >= kb1) {  // no update: beta * C
+        if (row_ok)
+          for (int j = 0; j < C::HALF; ++j) {
+            const long gj = gj0 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            float *cij = p.c + gi * p.rs_c + gj * p.cs_c;
+            *cij = p.beta != 0.f ? p.beta * *cij : 0.f;
+          }
+        continue;
+      }
+      const int nwin = (kb1 - kb0 + C::FLUSH - 1) / C::FLUSH;
+      float *crow = p.c + gi * p.rs_c;
+      for (int win = 0; win < nwin; ++win) {
+        if (win == nwin - 1 && row_ok && p.beta != 0.f) {
+#pragma unroll 8
+          for (int j = 0; j < C::HALF; ++j)
+            if (gj0 + j < w.n)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(crow + (gj0 + j) * p.cs_c));
+        }
+        int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
+        if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
+        tc::tc_fence_after();
+        const uint32_t base = lane_base + (uint32_t)(acc * C::TILE_N + half * C::HALF);
+#pragma unroll
+        for (int g0 = 0; g0 < C::HALF / 16; g0 += 4) {
+          uint32_t r[4][16];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tc::tmem_ld16(base + (uint32_t)((g0 + q) * 16), r[q]);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tc::tmem_tie16(r[q]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int c = (g0 + q) * 16 + j;
+              run[c] = win == 0 ? __uint_as_float(r[q][j])
+                                : __fadd_rn(run[c], __uint_as_float(r[q][j]));
+            }
+        }
+        tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive_cluster(tc::map_rank(&tempty[acc], 0));
+        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+      }
+      if (!ok) break;
+      if (row_ok) {
+        const int ei = F16 ? p.aexp[gi] : 0;
+#pragma unroll
+        for (int j0 = 0; j0 < C::HALF; j0 += 16) {
+          float cv[16];
+          int sc[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long gj = gj0 + j0 + j;
+            const bool in = gj < w.n && b200_rel(w.ji, gj, gi);
+            cv[j] = in && p.beta != 0.f ? crow[gj * p.cs_c] : 0.f;
+            sc[j] = F16 && in ? p.bexp[gj] : 0;
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long gj = gj0 + j0 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            float v = F16 ? p.alpha * b200_pow2_scale(run[j0 + j],
+                                                      ei + sc[j] - 2 * B200_FP16_SCALE_EXP)
+                          : p.alpha * run[j0 + j];
+            if (p.beta != 0.f) v = fmaf(p.beta, cv[j], v);
+            crow[gj * p.cs_c] = v;
+          }
+        }
+      }
+    }
+  }
+
+  // Both CTAs: every MMA has completed (the leader's issuer waited on the
+  // drain commit), every remote arrival has landed and no TMEM load is
+  // pending before the pair frees its TMEM.
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc_pair(tmem_base, C::TMEM_COLS);
+  }
+}
+
+template <int TERMS, int STAGES, bool F16 = false>
+int launch_bf16_pair(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &p,
+                     cudaStream_t s) {
+  using C = Bf16PairCfg<TERMS, STAGES>;
+  auto kern = tc_bf16_pair_kernel<TERMS, STAGES, F16>;
+  static bool configured = false;
+  static int max_clusters = 0;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(C::THREADS);
+  cfg.dynamicSmemBytes = C::SMEM;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (!configured) {
+    B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    cudaFuncAttributes fa;
+    B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
+      return b200_set_error(B200_EINVAL, "bf16 pair kernel: register split does not fit its launch");
+    cfg.gridDim = dim3(2 * b200_sm_count());
+    if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)kern, &cfg) != cudaSuccess ||
+        max_clusters < 1) {
+      cudaGetLastError();
+      return b200_set_error(B200_ECUDA, "bf16 pair kernel: no CTA pair can be resident");
+    }
+    configured = true;
+  }
+  const int tiles = p.w.tiles_m * p.w.tiles_n;
+  const int pairs = tiles < max_clusters ? tiles : max_clusters;
+  cfg.gridDim = dim3(2 * pairs);
+  B200ProfScope prof(F16 ? "tc_fp16x3" : (TERMS == 2 ? "tc_bf16x3" : "tc_bf16x6"), s);
+  B200_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, ta, tb, p));
+  return B200_OK;
+}
+
 template <int TERMS, int STAGES, bool F16 = false>
 int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &p,
                 cudaStream_t s) {
@@ -471,7 +782,14 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
   if (d->dtype != B200_F32) return b200_set_error(B200_EINVAL, "bf16 forms are FP32-only");
   const bool f16 = form == B200_FORM_FP16X3;
   const int terms = form == B200_FORM_BF16X6 ? 3 : 2;
-  constexpr int BM = 128, BN = 256, BK = 32;
+  // 256 x 256 tiles on CTA pairs (tc_bf16_pair_kernel) from 256 rows and
+  // columns on; MUBLIS_B200_TC_PAIR=0 keeps the single-SM kernel.
+  static const bool pair_on = [] {
+    const char *e = getenv("MUBLIS_B200_TC_PAIR");
+    return !(e && !strcmp(e, "0"));
+  }();
+  const bool pair = pair_on && d->m >= 256 && d->n >= 256;
+  const int BM = pair ? 256 : 128, BN = 256, BK = 32;
   cudaStream_t s = b200_cur_stream();
   const long ktot = (long)d->k * d->npairs;
   const long mpad = b200_round_up(d->m, BM), npad = b200_round_up(d->n, BN);
@@ -514,8 +832,9 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
     if (st == B200_OK) st = launch_pack<float>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
   }
   CUtensorMap ta, tb;
-  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 1, kpad, terms * mpad, BK, BM, 64);
-  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 1, kpad, terms * npad, BK, BN, 64);
+  // Boxes of one CTA's tile: 128 rows of A (both forms), 256 or 128 of B.
+  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 1, kpad, terms * mpad, BK, 128, 64);
+  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 1, kpad, terms * npad, BK, pair ? 128 : BN, 64);
   if (st == B200_OK) {
     Bf16Params p;
     p.w.tiles_m = (int)(mpad / BM);
@@ -540,8 +859,13 @@ int tc_run_bf16(const b200_l3_desc_t *d, int form) {
     p.err = b200_device_error_word();
     p.aexp = ae;
     p.bexp = ae ? ae + mpad : nullptr;
-    st = f16 ? launch_bf16<2, 4, true>(ta, tb, p, s)
-             : (terms == 2 ? launch_bf16<2, 4>(ta, tb, p, s) : launch_bf16<3, 3>(ta, tb, p, s));
+    if (pair)
+      st = f16 ? launch_bf16_pair<2, 6, true>(ta, tb, p, s)
+               : (terms == 2 ? launch_bf16_pair<2, 6>(ta, tb, p, s)
+                             : launch_bf16_pair<3, 4>(ta, tb, p, s));
+    else
+      st = f16 ? launch_bf16<2, 4, true>(ta, tb, p, s)
+               : (terms == 2 ? launch_bf16<2, 4>(ta, tb, p, s) : launch_bf16<3, 3>(ta, tb, p, s));
   }
   b200_free(ap);
   b200_free(bp);
