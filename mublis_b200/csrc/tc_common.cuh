@@ -339,6 +339,17 @@ __device__ __forceinline__ void mma_f16_pair(uint32_t d_tmem, uint64_t a_desc, u
       : "memory");
 }
 
+// Leader: D (+)= A * B^T in int8 with exact int32 accumulation, M = 256.
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 // Leader: arrive on the barrier at this shared offset in both CTAs once the
 // issued MMAs have completed.
 __device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {

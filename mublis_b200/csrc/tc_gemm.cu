@@ -1306,6 +1306,298 @@ __global__ void __launch_bounds__(384, 1)
   }
 }
 
+// ---- modular form on CTA pairs ------------------------------------------------
+//
+// tc_ozaki_kernel<true> with the 256 x 256 tile on a pair of SMs (cluster
+// of two, cta_group::2): each CTA loads its 128 rows of op(A) and 128 rows
+// (tile columns) of op(B) into its own shared memory, the leader issues one
+// M = 256, N = 256 int8 MMA per k-step, and each CTA's TMEM holds its 128
+// accumulator rows x 256 columns -- half of what one CTA of the single-SM
+// kernel needs, so two accumulators fit and the epilogue's reduction of
+// modulus l overlaps the MMAs of modulus l + 1 (the single-SM kernel's
+// issuer waits for every drain).  Residues, CRT and the output are the
+// single-SM kernel's, element by element.
+struct OzPairCfg {
+  static constexpr int BM = 128, BN = 128, SWZ = 128, BK = 128, STAGES = 6;  // per CTA
+  static constexpr int TILE_M = 256, TILE_N = 256;
+  static constexpr int A_TILE = BM * SWZ, B_TILE = BN * SWZ;
+  static constexpr int STAGE_BYTES = A_TILE + B_TILE;
+  static constexpr int KSTEPS = SWZ / 32;
+  static constexpr int THREADS = 384, EPI_WARPS = 8;
+  static constexpr int HALF = TILE_N / 2;  // columns per epilogue thread
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr uint32_t TMEM_COLS = 512;
+};
+
+template <typename TC>
+__global__ void __launch_bounds__(384, 1)
+    tc_ozaki2_pair_kernel(const __grid_constant__ CUtensorMap tmA,
+                          const __grid_constant__ CUtensorMap tmB, const __grid_constant__ OzParams p) {
+  using C = OzPairCfg;
+  constexpr int STAGES = C::STAGES;
+  constexpr int KCHUNK = OZ2_KCHUNK / C::BK;  // in k-blocks
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem =
+      (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + STAGES * C::STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *tfull = empty + STAGES;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = tc::cluster_rank();
+  const bool leader = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      tc::mbar_init(&tfull[a], 1);
+      tc::mbar_init(&tempty[a], 2 * C::EPI_WARPS);
+    }
+    tc::mbar_init(drain, 1);
+    *abort_flag = 0;
+    tc::fence_barrier_init();
+    tc::tma_prefetch_desc(&tmA);
+    tc::tma_prefetch_desc(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc_pair(tmem_slot, C::TMEM_COLS);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const TileWalk &w = p.w;  // bm = bn = 256: pair tiles
+  const int S = p.slices;   // modulus count
+  const int num_tiles = w.tiles_m * w.tiles_n;
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  auto sa = [&](int st) { return smem + st * C::STAGE_BYTES; };
+  auto sb = [&](int st) { return smem + st * C::STAGE_BYTES + C::A_TILE; };
+
+  if (warp < 4) {
+  tc::setmaxnreg_dec<TC_PRODUCER_REGS>();
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    int stage = 0, issued = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const long arow = (long)tm * C::TILE_M + rank * C::BM;
+      const long brow = (long)tn * C::TILE_N + rank * C::BN;
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += KCHUNK) {
+        const int c1 = min(kb1, c0 + KCHUNK);
+        for (int l = 0; l < S && ok; ++l) {
+          for (int kb = c0; kb < c1; ++kb) {
+            if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+            if (leader) tc::mbar_arrive_expect_tx(&full[stage], 2 * C::STAGE_BYTES);
+            const uint32_t fb = tc::map_rank(&full[stage], 0);
+            tc::tma_load_2d_pair(sa(stage), &tmA, fb, kb * C::BK, (int)(l * p.mpad + arow));
+            tc::tma_load_2d_pair(sb(stage), &tmB, fb, kb * C::BK, (int)(l * p.npad + brow));
+            ++issued;
+            if (++stage == STAGES) { stage = 0; phase ^= 1; }
+          }
+        }
+      }
+    }
+    if (leader) {  // both CTAs' last loads complete on the leader's barriers
+      int pending = issued < STAGES ? issued : STAGES;
+      for (int q = 0; q < pending; ++q) {
+        if (--stage < 0) { stage = STAGES - 1; phase ^= 1; }
+        if (!tc::mbar_wait_drain(&full[stage], phase)) break;
+      }
+    }
+  } else if (warp == 1 && lane == 0 && leader) {
+    // ---------------- MMA issuer (leader) ----------------
+    constexpr uint32_t IDESC = tc::idesc_s8(C::TILE_M, C::TILE_N);
+    int stage = 0, acc = 0;
+    uint32_t phase = 0, acc_phase = 0;
+    bool ok = true, any = false;
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      for (int c0 = kb0; c0 < kb1 && ok; c0 += KCHUNK) {
+        const int c1 = min(kb1, c0 + KCHUNK);
+        for (int l = 0; l < S && ok; ++l) {
+          // Both CTAs' epilogues have reduced this accumulator's last use.
+          if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag, p.err)) { ok = false; break; }
+          tc::tc_fence_after();
+          const uint32_t d = tmem_base + (uint32_t)(acc * C::TILE_N);
+          bool first = true;
+          for (int kb = c0; kb < c1; ++kb) {
+            if (!tc::mbar_wait(&full[stage], phase, abort_flag, p.err)) { ok = false; break; }
+            tc::tc_fence_after();
+            const uint64_t ad = tc::smem_desc(sa(stage), C::SWZ);
+            const uint64_t bd = tc::smem_desc(sb(stage), C::SWZ);
+#pragma unroll
+            for (int ks = 0; ks < C::KSTEPS; ++ks) {
+              const uint64_t off = (uint64_t)((ks * 32) >> 4);
+              tc::mma_i8_pair(d, ad + off, bd + off, IDESC, first ? 0u : 1u);
+              first = false;
+            }
+            tc::mma_commit_pair(&empty[stage]);
+            any = true;
+            if (++stage == STAGES) { stage = 0; phase ^= 1; }
+          }
+          if (!ok) break;
+          tc::mma_commit_pair(&tfull[acc]);
+          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+      }
+    }
+    if (any) {
+      tc::mma_commit_pair(drain);
+      tc::mbar_wait(drain, 0, abort_flag, p.err);
+    }
+  }
+  } else {
+    tc::setmaxnreg_inc<TC_EPILOGUE_REGS>();
+    // ---------------- epilogue (both CTAs: this CTA's 128 rows) ----------------
+    // Warps 4-7 take columns 0-127 of the tile, warps 8-11 columns 128-255;
+    // each warp reads the TMEM lanes of its quadrant.
+    const int quad = warp & 3, hc = (warp - 4) >> 2;
+    const int row = quad * 32 + lane;  // row within this CTA's half of the tile
+    const uint32_t lane_base = tmem_base + ((uint32_t)(quad * 32) << 16) + (uint32_t)(hc * C::HALF);
+    // Residue workspace: [l][16-column chunk][row][16 B] for this CTA's 128
+    // rows, so a warp's 16-byte stores and loads are 512 contiguous bytes.
+    unsigned char *R = (unsigned char *)p.work + (size_t)blockIdx.x * S * C::BM * C::TILE_N;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    for (int idx = pair; idx < num_tiles && ok; idx += npairs) {
+      int tm, tn, kb0, kb1;
+      w.coords(idx, tm, tn);
+      if (!w.valid(tm, tn)) continue;
+      w.krange(tm, tn, kb0, kb1);
+      const long gi = (long)tm * C::TILE_M + rank * C::BM + row;
+      const bool row_ok = gi < w.m;
+      const int ei = row_ok ? p.aexp[gi] : 0;
+      const long gj0 = (long)tn * C::TILE_N + hc * C::HALF;
+      if (kb0 >= kb1) {  // no update: beta * C
+        if (row_ok)
+          for (int j = 0; j < C::HALF; ++j) {
+            const long gj = gj0 + j;
+            if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+            TC *cij = (TC *)p.c + gi * p.rs_c + gj * p.cs_c;
+            *cij = p.beta != 0.0 ? (TC)(p.beta * (double)*cij) : TC(0);
+          }
+        continue;
+      }
+      const int nchunks = (kb1 - kb0 + KCHUNK - 1) / KCHUNK;
+      for (int cc = 0; cc < nchunks && ok; ++cc) {
+        for (int l = 0; l < S; ++l) {
+          int wok = tc::mbar_wait(&tfull[acc], acc_phase, abort_flag, p.err);
+          if (!__all_sync(0xffffffffu, wok)) { ok = false; break; }
+          tc::tc_fence_after();
+          const int m = p.crt.m[l], bias = p.crt.bias[l];
+          const unsigned mg = p.crt.mg[l];
+          uint4 *Rl = (uint4 *)(R + (size_t)l * C::BM * C::TILE_N) + row;
+          const uint32_t base = lane_base + (uint32_t)(acc * C::TILE_N);
+#pragma unroll
+          for (int ch0 = 0; ch0 < C::HALF / 16; ch0 += 4) {
+            uint32_t rb[4][16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) tc::tmem_ld16(base + (uint32_t)((ch0 + q) * 16), rb[q]);
+            const int chunk0 = hc * (C::HALF / 16) + ch0;  // 16-column chunk of the tile
+            uint4 prev[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              prev[q] = cc > 0 ? Rl[(chunk0 + q) * C::BM] : make_uint4(0, 0, 0, 0);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 4; ++q) tc::tmem_tie16(rb[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              uint32_t out[4] = {0, 0, 0, 0};
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                int res = b200_sym_mod((int)rb[q][j], m, mg, bias);  // |C'_l| <= 2^29
+                if (cc > 0) {
+                  const uint4 pv = prev[q];
+                  const uint32_t word = j < 4 ? pv.x : j < 8 ? pv.y : j < 12 ? pv.z : pv.w;
+                  res = b200_sym_mod(res + (int)(int8_t)(word >> (8 * (j & 3))), m, mg, bias);
+                }
+                out[j >> 2] |= (uint32_t)(res & 0xff) << (8 * (j & 3));
+              }
+              Rl[(chunk0 + q) * C::BM] = make_uint4(out[0], out[1], out[2], out[3]);
+            }
+          }
+          tc::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive_cluster(tc::map_rank(&tempty[acc], 0));
+          if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+      }
+      // The tile's accumulators are released; reconstruct C' from this
+      // thread's own residues while the MMAs of the next tile run.
+      if (!ok || !row_ok) continue;
+      const OzCrt &k = p.crt;
+      const int sh = ei - k.bits;
+#pragma unroll 1
+      for (int ch8 = 0; ch8 < C::HALF / 8; ++ch8) {
+        double s0[8], s1[8], s2[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s0[j] = s1[j] = s2[j] = 0.0;
+        const int col8 = hc * (C::HALF / 8) + ch8;  // 8-column group of the tile
+        const uint2 *rbase =
+            (const uint2 *)((const uint4 *)R + (size_t)(col8 >> 1) * C::BM + row) + (col8 & 1);
+        uint2 rv[B200_MAX_MODULI];
+#pragma unroll
+        for (int l = 0; l < B200_MAX_MODULI; ++l)
+          rv[l] = l < S ? rbase[(size_t)l * (C::BM * C::TILE_N / 8)] : make_uint2(0, 0);
+        TC cv[8];
+        int sc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const long gj = gj0 + ch8 * 8 + j;
+          const bool in = gj < w.n && b200_rel(w.ji, gj, gi);
+          cv[j] = in && p.beta != 0.0 ? ((const TC *)p.c)[gi * p.rs_c + gj * p.cs_c] : TC(0);
+          sc[j] = in ? p.bexp[gj] : 0;
+        }
+#pragma unroll
+        for (int l = 0; l < B200_MAX_MODULI; ++l) {
+          if (l >= S) break;
+          const uint2 v = rv[l];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const double rr = (double)(int8_t)((j < 4 ? v.x : v.y) >> (8 * (j & 3)));
+            s0[j] = fma(rr, k.w[l][0], s0[j]);
+            s1[j] = fma(rr, k.w[l][1], s1[j]);
+            s2[j] = fma(rr, k.w[l][2], s2[j]);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const long gj = gj0 + ch8 * 8 + j;
+          if (gj >= w.n || !b200_rel(w.ji, gj, gi)) continue;
+          const double cp = oz_crt(k, s0[j], s1[j], s2[j]);
+          double out = p.alpha * b200_pow2_scale(cp, sh + sc[j]);
+          if (p.beta != 0.0) out = fma(p.beta, (double)cv[j], out);
+          ((TC *)p.c)[gi * p.rs_c + gj * p.cs_c] = (TC)out;
+        }
+      }
+    }
+  }
+
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::cluster_sync();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc_pair(tmem_base, C::TMEM_COLS);
+  }
+}
+
 // The modular form's moduli: the largest pairwise coprime integers <= 256.
 constexpr int OZ2_MODULI[B200_MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233,
                                              229, 227, 223, 217, 211, 199, 197, 193};
@@ -1358,6 +1650,60 @@ int oz2_setup(int N, long k, int pmax, B200Moduli *mod, OzCrt *crt, int *pa, int
 namespace {
 
 template <typename T>
+cudaLaunchConfig_t oz2_pair_config(cudaLaunchAttribute *attr, int grid, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(OzPairCfg::THREADS);
+  cfg.dynamicSmemBytes = OzPairCfg::SMEM;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// Configures the pair kernel once (shared memory, register-split check) and
+// returns how many CTA pairs can be resident at once.
+template <typename T>
+int oz2_pair_clusters(int *clusters) {
+  static int cached = 0;
+  if (cached > 0) {
+    *clusters = cached;
+    return B200_OK;
+  }
+  auto kern = tc_ozaki2_pair_kernel<T>;
+  B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     OzPairCfg::SMEM));
+  cudaFuncAttributes fa;
+  B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+  if (OzPairCfg::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
+    return b200_set_error(B200_EINVAL, "ozaki2 pair kernel: register split does not fit its launch");
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = oz2_pair_config<T>(attr, 2 * b200_sm_count(), nullptr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    return b200_set_error(B200_ECUDA, "ozaki2 pair kernel: no CTA pair can be resident");
+  }
+  cached = n;
+  *clusters = n;
+  return B200_OK;
+}
+
+template <typename T>
+int launch_oz2_pair(const CUtensorMap &ta, const CUtensorMap &tb, const OzParams &p, int grid,
+                    cudaStream_t s) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = oz2_pair_config<T>(attr, grid, s);
+  B200ProfScope prof(sizeof(T) == 8 ? "tc_ozaki2_i8" : "tc_ozaki2_s_i8", s);
+  B200_CUDA_TRY(cudaLaunchKernelEx(&cfg, tc_ozaki2_pair_kernel<T>, ta, tb, p));
+  return B200_OK;
+}
+
+template <typename T>
 int run_ozaki(const b200_l3_desc_t *d, bool mod) {
   using C = OzCfg;
   constexpr bool F64 = sizeof(T) == 8;
@@ -1383,7 +1729,23 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
   if (mod) B200_TRY(oz2_setup(slices, ktot, F64 ? 56 : 27, &moduli, &p.crt, &pa, &pb));
   const int sms = b200_sm_count();
   const int tiles = (int)((mpad / C::BM) * (npad / C::BN));
-  const int grid = tiles < sms ? tiles : sms;
+  // The modular form runs on CTA pairs (tc_ozaki2_pair_kernel) below 576
+  // tiles (24^2: up to ~6000^2 outputs), unless MUBLIS_B200_TC_PAIR=0; grid
+  // then counts CTAs, two per tile slot.  Measured kernel times, pair vs
+  // one SM per tile: 2048^3 0.18 vs 0.38 ms (the 64 tiles keep 128 SMs busy
+  // instead of 64), 3072^3 0.43 vs 0.48, 4096^3 1.02 vs 1.09, 6144^3 2.90
+  // vs 2.91, 8192^3 6.70 vs 6.45.  Results are bit-identical either way.
+  static const bool pair_on = [] {
+    const char *e = getenv("MUBLIS_B200_TC_PAIR");
+    return !(e && !strcmp(e, "0"));
+  }();
+  const bool pair = mod && pair_on && tiles < 576;
+  int grid = tiles < sms ? tiles : sms;
+  if (pair) {
+    int clusters = 0;
+    B200_TRY(oz2_pair_clusters<T>(&clusters));
+    grid = 2 * (tiles < clusters ? tiles : clusters);
+  }
 
   void *ap = nullptr, *bp = nullptr, *amax = nullptr, *bmax = nullptr, *work = nullptr;
   int st = b200_alloc(&amax, (sizeof(unsigned long long) + sizeof(int)) * (mpad + npad));
@@ -1397,8 +1759,9 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
   }
   if (st == B200_OK) st = b200_alloc(&ap, (size_t)slices * mpad * kpad);
   if (st == B200_OK) st = b200_alloc(&bp, (size_t)slices * npad * kpad);
-  const size_t work_bytes = mod ? (size_t)grid * slices * C::BM * C::BN
-                                : sizeof(double) * grid * C::BM * C::BN;
+  const size_t work_bytes = pair ? (size_t)grid * slices * OzPairCfg::BM * OzPairCfg::TILE_N
+                            : mod  ? (size_t)grid * slices * C::BM * C::BN
+                                   : sizeof(double) * grid * C::BM * C::BN;
   if (st == B200_OK) st = b200_alloc(&work, work_bytes);
   const mublis_l3_product_t &pr = d->product;
   PackView va[2], vb[2];
@@ -1426,8 +1789,10 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
     if (st == B200_OK) st = launch_pack<T>(vb[t], true, d->n, d->k, npad, kk0, kk1, ob, s);
   }
   CUtensorMap ta, tb;
-  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 0, kpad, slices * mpad, C::BK, C::BM, C::SWZ);
-  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 0, kpad, slices * npad, C::BK, C::BN, C::SWZ);
+  // Boxes of one CTA's share of a tile: 256 rows, or 128 on CTA pairs.
+  const int box = pair ? OzPairCfg::BM : C::BM;
+  if (st == B200_OK) st = b200_make_tmap(&ta, ap, 0, kpad, slices * mpad, C::BK, box, C::SWZ);
+  if (st == B200_OK) st = b200_make_tmap(&tb, bp, 0, kpad, slices * npad, C::BK, box, C::SWZ);
   if (st == B200_OK) {
     p.w.tiles_m = (int)(mpad / C::BM);
     p.w.tiles_n = (int)(npad / C::BN);
@@ -1453,6 +1818,14 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
     p.aexp = exps;
     p.bexp = exps + mpad;
     p.err = b200_device_error_word();
+    if (pair) {
+      st = launch_oz2_pair<T>(ta, tb, p, grid, s);
+      b200_free(ap);
+      b200_free(bp);
+      b200_free(work);
+      b200_free(amax);
+      return st;
+    }
     auto kern = tc_ozaki_kernel<true, T>;
     if constexpr (F64) {
       if (!mod) kern = tc_ozaki_kernel<false, double>;
