@@ -495,7 +495,7 @@ def _log_uniform_int(rng, lo, hi, size):
 
 
 def _grouped_sgemms(torch, rng):
-    """Config 4's 4096 SGEMMs on the device: (problems, operand tensors, ctypes array)."""
+    """The grouped study's 4096 SGEMMs on the device: (problems, operand tensors, ctypes array)."""
     import mublis_b200 as mb
     torch.manual_seed(1)
     mnk = _log_uniform_int(rng, 16, 512, (4096, 3))
@@ -513,7 +513,7 @@ def _grouped_sgemms(torch, rng):
 
 
 def grouped_direct(torch, lib, form: str = "plain") -> dict:
-    """Config 4's SGEMMs as direct grouped calls (no plan, no autotuning) in
+    """The grouped study's SGEMMs as direct grouped calls (no plan, no autotuning) in
     the given FP32 form: one warm-up call, then five timed (plain: three
     kernel launches per call, one per tile class; fp16x3: a pack and one
     tensor-core launch).  For profiler captures of the grouped kernels."""
@@ -531,7 +531,7 @@ def grouped_direct(torch, lib, form: str = "plain") -> dict:
 
 
 def grouped_study(torch, lib) -> dict:
-    """Config 4: 4096 independent SGEMMs with m, n, k log-uniform over [16, 512]
+    """Grouped study: 4096 independent SGEMMs with m, n, k log-uniform over [16, 512]
     (seed 1), column-major, lda = m, per-problem alpha, beta uniform[0.5, 1.5);
     and 1024 DTRSMs (left, lower, non-unit) with order log-uniform in [32, 256],
     right-hand sides log-uniform in [1, 128], A off-diagonal uniform/n and
@@ -596,7 +596,7 @@ def grouped_study(torch, lib) -> dict:
 
 
 def served_study(torch, lib, nreq: int = 4000, ring: int = 8) -> dict:
-    """Config 5: 16 host threads issue cblas calls with Poisson arrivals
+    """Served study: 16 host threads issue cblas calls with Poisson arrivals
     (aggregate 20k calls/s, seed 2); mix 60% SGEMM, 20% DGEMM, 10% SSYRK, 10%
     DTRSM; 80% of sizes log-uniform in [32, 256], 20% from {1024, 2048, 4096,
     8192}; operands device-resident in server handles under a 64 GiB HBM
@@ -781,14 +781,14 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the 8192 precision-form study")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-studies", action="store_true",
-                    help="skip the grouped (config 4) and served (config 5) studies")
+                    help="skip the grouped (4096 small GEMMs) and served (4000-request mix) studies")
     ap.add_argument("--only-forms", action="store_true",
                     help="run only the precision-form study (for profiler captures)")
     ap.add_argument("--forms-n", type=int, default=8192)
     ap.add_argument("--only-sides", action="store_true",
                     help="run only the TRSM/TRMM side x uplo x transpose study")
     ap.add_argument("--only-grouped", action="store_true",
-                    help="run only config 4's SGEMMs as direct grouped calls (profiler captures)")
+                    help="run only the grouped study's SGEMMs as direct grouped calls (profiler captures)")
     ap.add_argument("--grouped-form", default="plain", choices=["plain", "fp16x3"],
                     help="FP32 form of --only-grouped")
     ap.add_argument("--only-trsm", default=None, choices=["s", "d"],
@@ -989,9 +989,9 @@ def main():
                 "clocks": clocks, "gpu_launches": int(launches), "breakdown_tflops": breakdown,
                 "verified": verified,
                 "stated_err": "normwise relative error <= 4*k*u against the oracle "
-                              "(tests/test_gpu_config2.py checks this workload's 18 calls); "
+                              "(tests/test_gpu_family_n4096.py checks this workload's 18 calls); "
                               "measured plain SGEMM ~1.9e-8, DGEMM ~3.4e-17 at 8192",
-                "forms_8192_tflops": forms, "grouped_config4": grouped, "served_config5": served,
+                "forms_8192_tflops": forms, "grouped_study": grouped, "served_study": served,
                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in kstats.items()}}
         print(json.dumps(line))
     if world > 1:

@@ -312,7 +312,7 @@ def test_dtrsm_8192_forms(lib):
 
 @pytest.mark.parametrize("kind", [orc.UNIFORM, orc.WIDE], ids=["uniform", "wide"])
 def test_ozaki2_autotune_picks_fewest_moduli_for_target(lib, kind):
-    """mublis_b200_ozaki2_autotune (config 3b: the modulus count chosen for a
+    """mublis_b200_ozaki2_autotune (the modulus count chosen for a
     stated error): a looser target never takes more moduli than a tighter
     one, the measured calibration error of the choice meets the target
     (unless all 16 moduli were needed), and a call with form

@@ -1,4 +1,4 @@
-"""Grouped launches (config 4 style): many independent GEMMs / TRSMs of
+"""Grouped launches: many independent GEMMs / TRSMs of
 uneven sizes in one persistent launch, and plans (autotuned tiles + CUDA
 graph replay).
 

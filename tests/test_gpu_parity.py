@@ -291,7 +291,7 @@ def test_device_pointers_in_place(lib):
     assert cs.normwise_error(case, out, ref, a, b, c0) <= tol_of(case)
 
 
-def test_config1_sgemm_1024(lib):
+def test_sgemm_1024_seeded_case(lib):
     """Plain SGEMM NN, column-major, m=n=k=1024, alpha 1, beta 0.5, seed 0:
     normwise error <= 4 * 1024 * 2^-24 against the oracle."""
     case = dict(routine="gemm", dtype="float32", order="F", m=1024, n=1024, k=1024, ta=False,
