@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "b200_internal.h"
 
 #define B200_CUDA_TRY(expr)                                                   \
@@ -37,6 +39,16 @@ struct B200ProfScope {
   B200ProfScope(const char *name, cudaStream_t s);
   ~B200ProfScope();
 };
+
+// Runs `setup` once per process: callers that arrive while it runs wait for
+// it, and every caller gets its status (with a last-error message of its own
+// when it failed: `what`).  For one-time kernel attribute set-up that several
+// host threads may reach first at the same time.
+template <class F>
+int b200_once(std::once_flag &flag, int &status, const char *what, F setup) {
+  std::call_once(flag, [&] { status = setup(); });
+  return status == B200_OK ? B200_OK : b200_set_error(status, what);
+}
 
 static inline long b200_round_up(long x, long m) { return (x + m - 1) / m * m; }
 static inline long b200_ceil_div(long x, long m) { return (x + m - 1) / m; }

@@ -321,11 +321,12 @@ __global__ void __launch_bounds__(THREADS, 1)
 template <bool DIRECT, bool A_KC, bool B_KC>
 int launch_variant(const DmmaGemmArgs &a, int grid, cudaStream_t s) {
   auto kern = dmma_gemm_kernel<DIRECT, A_KC, B_KC>;
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag once;
+  static int conf = B200_OK;
+  B200_TRY(b200_once(once, conf, "dmma kernel: set-up failed", [&]() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
-    configured = true;
-  }
+    return B200_OK;
+  }));
   B200ProfScope prof("dmma_dgemm", s);
   kern<<<grid, THREADS, SMEM, s>>>(a);
   B200_LAUNCH_CHECK();

@@ -638,12 +638,13 @@ int launch_trsm_group(TrsmGroup &g, cudaStream_t s) {
   if (g.slabs == 0) return B200_OK;
   const int grid = std::min(g.slabs, sm_count() * 4);
   const size_t smem = sizeof(T) * (TRSM_MAX_ORDER * (TRSM_SLAB + 1) + 32 * 33);
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag once;
+  static int conf = B200_OK;
+  B200_TRY(b200_once(once, conf, "grouped trsm: set-up failed", [&]() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(grouped_trsm_kernel<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+    return B200_OK;
+  }));
   B200ProfScope prof(sizeof(T) == 4 ? "grouped_strsm" : "grouped_dtrsm", s);
   grouped_trsm_kernel<T><<<grid, 256, smem, s>>>(g.dtable, (int)g.entries.size(), g.slabs);
   B200_LAUNCH_CHECK();

@@ -706,8 +706,8 @@ int launch_bf16_pair(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Par
                      cudaStream_t s) {
   using C = Bf16PairCfg<TERMS, STAGES>;
   auto kern = tc_bf16_pair_kernel<TERMS, STAGES, F16>;
-  static bool configured = false;
-  static int max_clusters = 0;
+  static std::once_flag once;
+  static int conf = B200_OK, max_clusters = 0;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -719,20 +719,21 @@ int launch_bf16_pair(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Par
   cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (!configured) {
+  B200_TRY(b200_once(once, conf, "bf16 pair kernel: set-up failed", [&]() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
     cudaFuncAttributes fa;
     B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
     if (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
       return b200_set_error(B200_EINVAL, "bf16 pair kernel: register split does not fit its launch");
-    cfg.gridDim = dim3(2 * b200_sm_count());
-    if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)kern, &cfg) != cudaSuccess ||
+    cudaLaunchConfig_t q = cfg;
+    q.gridDim = dim3(2 * b200_sm_count());
+    if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)kern, &q) != cudaSuccess ||
         max_clusters < 1) {
       cudaGetLastError();
       return b200_set_error(B200_ECUDA, "bf16 pair kernel: no CTA pair can be resident");
     }
-    configured = true;
-  }
+    return B200_OK;
+  }));
   const int tiles = p.w.tiles_m * p.w.tiles_n;
   const int pairs = tiles < max_clusters ? tiles : max_clusters;
   cfg.gridDim = dim3(2 * pairs);
@@ -746,8 +747,9 @@ int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &
                 cudaStream_t s) {
   using C = Bf16Cfg<TERMS, STAGES>;
   auto kern = tc_bf16_kernel<TERMS, STAGES, F16>;
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag once;
+  static int conf = B200_OK;
+  B200_TRY(b200_once(once, conf, "bf16 kernel: set-up failed", [&]() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
     // The warpgroup register split assumes this launch allocation; with
     // fewer registers per thread the epilogue's increase could never be
@@ -756,8 +758,8 @@ int launch_bf16(const CUtensorMap &ta, const CUtensorMap &tb, const Bf16Params &
     B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
     if (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
       return b200_set_error(B200_EINVAL, "bf16 kernel: register split does not fit its launch");
-    configured = true;
-  }
+    return B200_OK;
+  }));
   const int sms = b200_sm_count();
   int tiles = p.w.tiles_m * p.w.tiles_n;
   int grid = tiles < sms ? tiles : sms;
@@ -1669,27 +1671,25 @@ cudaLaunchConfig_t oz2_pair_config(cudaLaunchAttribute *attr, int grid, cudaStre
 // returns how many CTA pairs can be resident at once.
 template <typename T>
 int oz2_pair_clusters(int *clusters) {
-  static int cached = 0;
-  if (cached > 0) {
-    *clusters = cached;
+  static std::once_flag once;
+  static int conf = B200_OK, cached = 0;
+  B200_TRY(b200_once(once, conf, "ozaki2 pair kernel: set-up failed", []() -> int {
+    auto kern = tc_ozaki2_pair_kernel<T>;
+    B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       OzPairCfg::SMEM));
+    cudaFuncAttributes fa;
+    B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+    if (OzPairCfg::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
+      return b200_set_error(B200_EINVAL, "ozaki2 pair kernel: register split does not fit its launch");
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = oz2_pair_config<T>(attr, 2 * b200_sm_count(), nullptr);
+    if (cudaOccupancyMaxActiveClusters(&cached, (void *)kern, &cfg) != cudaSuccess || cached < 1) {
+      cudaGetLastError();
+      return b200_set_error(B200_ECUDA, "ozaki2 pair kernel: no CTA pair can be resident");
+    }
     return B200_OK;
-  }
-  auto kern = tc_ozaki2_pair_kernel<T>;
-  B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     OzPairCfg::SMEM));
-  cudaFuncAttributes fa;
-  B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
-  if (OzPairCfg::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
-    return b200_set_error(B200_EINVAL, "ozaki2 pair kernel: register split does not fit its launch");
-  cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = oz2_pair_config<T>(attr, 2 * b200_sm_count(), nullptr);
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg) != cudaSuccess || n < 1) {
-    cudaGetLastError();
-    return b200_set_error(B200_ECUDA, "ozaki2 pair kernel: no CTA pair can be resident");
-  }
-  cached = n;
-  *clusters = n;
+  }));
+  *clusters = cached;
   return B200_OK;
 }
 
@@ -1830,20 +1830,20 @@ int run_ozaki(const b200_l3_desc_t *d, bool mod) {
     if constexpr (F64) {
       if (!mod) kern = tc_ozaki_kernel<false, double>;
     }
-    static bool configured[2] = {false, false};
-    if (!configured[mod]) {
-      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) !=
-          cudaSuccess)
-        st = b200_set_error(B200_ECUDA, "ozaki: smem attribute");
-      // The warpgroup register split must fit the compiled allocation (an
-      // increase that cannot be granted would wait forever).
-      cudaFuncAttributes fa;
-      if (st == B200_OK && cudaFuncGetAttributes(&fa, kern) != cudaSuccess)
-        st = b200_set_error(B200_ECUDA, "ozaki: function attributes");
-      if (st == B200_OK && (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs)))
-        st = b200_set_error(B200_EINVAL, "ozaki kernel: register split does not fit its launch");
-      configured[mod] = st == B200_OK;
-    }
+    static std::once_flag once[2];
+    static int conf[2] = {B200_OK, B200_OK};
+    if (st == B200_OK)
+      st = b200_once(once[mod], conf[mod], "ozaki kernel: set-up failed", [&]() -> int {
+        B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           C::SMEM));
+        // The warpgroup register split must fit the compiled allocation (an
+        // increase that cannot be granted would wait forever).
+        cudaFuncAttributes fa;
+        B200_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+        if (C::THREADS != 384 || !tc_register_split_fits(fa.numRegs))
+          return b200_set_error(B200_EINVAL, "ozaki kernel: register split does not fit its launch");
+        return B200_OK;
+      });
     if (st == B200_OK) {
       B200ProfScope prof(mod ? (F64 ? "tc_ozaki2_i8" : "tc_ozaki2_s_i8") : "tc_ozaki_i8", s);
       kern<<<grid, C::THREADS, C::SMEM, s>>>(ta, tb, p);

@@ -711,8 +711,9 @@ int b200_tcg_create(const mublis_b200_gemm_problem_t *p, int count, b200_tcg **o
 }
 
 int b200_tcg_run(b200_tcg *g, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
+  static std::once_flag once;
+  static int conf = B200_OK;
+  B200_TRY(b200_once(once, conf, "grouped fp16x3 kernels: set-up failed", []() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(tcg_pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(float) * TCG_PACK_NBUF * 32 * (TCG_PACK_KS + 1))));
     B200_CUDA_TRY(cudaFuncSetAttribute(tcg_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -725,8 +726,8 @@ int b200_tcg_run(b200_tcg *g, cudaStream_t s) {
     if (fa.numRegs < TCG_PRODUCER_REGS ||
         128L * (fa.numRegs - TCG_PRODUCER_REGS) < 256L * (TCG_EPILOGUE_REGS - fa.numRegs))
       return b200_set_error(B200_EINVAL, "grouped fp16x3 kernel: register split does not fit");
-    configured = true;
-  }
+    return B200_OK;
+  }));
   if (g->ntasks > 0) {
     const int ks = std::min(g->kpad_max, TCG_PACK_KS);
     const size_t smem = sizeof(float) * TCG_PACK_NBUF * 32 * (ks + 1);

@@ -498,13 +498,14 @@ template <typename T>
 int leaf_solve(const void *pack, int rows, T *b, long rs_b, long cs_b, int n) {
   if (rows <= 0 || n <= 0) return B200_OK;
   cudaStream_t s = b200_cur_stream();
-  static bool configured = false;
+  static std::once_flag once;
+  static int conf = B200_OK;
   constexpr size_t smem = leaf_smem<T>();
-  if (!configured) {
+  B200_TRY(b200_once(once, conf, "trsm leaf kernel: set-up failed", []() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(trsm_leaf_kernel<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+    return B200_OK;
+  }));
   LeafArgs<T> la{(const T *)pack, rows, b, rs_b, cs_b, n, b200_device_error_word(), B200_WAIT_NS};
   const long grid = b200_ceil_div(n, NBC);
   if (grid > 0x7fffffffL) return b200_set_error(B200_EINVAL, "trsm: too many right-hand sides");
