@@ -485,13 +485,15 @@ int launch_cfg(const SimtGemmArgs<T> &a0, cudaStream_t s, const SimtPolicy *pol)
   auto kern = simt_tile_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR>;
   auto kern_split = simt_gemm_kernel<T, BM, BN, BK, WM, WN, ST, MINB, PAIR, true>;
   const size_t smem = (size_t)ST * BK * (BM + BN) * sizeof(T);
-  static int per_sm = 0;
-  if (!per_sm) {
+  static std::once_flag once;
+  static int conf = B200_OK, per_sm = 0;
+  B200_TRY(b200_once(once, conf, "gemm: set-up failed", [&]() -> int {
     B200_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     B200_CUDA_TRY(
         cudaFuncSetAttribute(kern_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     per_sm = std::min(resident_per_sm(kern, smem), resident_per_sm(kern_split, smem));
-  }
+    return B200_OK;
+  }));
   const long tiles = b200_ceil_div(a0.m, BM) * b200_ceil_div(a0.n, BN);
   if (tiles <= 0) return B200_OK;
   if (tiles > 0x7fffffffL / 16) return b200_set_error(B200_EINVAL, "gemm: too many tiles");
